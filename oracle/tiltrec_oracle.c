@@ -1,0 +1,126 @@
+/* CPU restatement of the reference TiltRec path (the oracle).
+ * TEST INFRASTRUCTURE: see tiltrec_oracle.h for who may load it and how it
+ * is pinned against the reference. */
+#include "tiltrec_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* PI_180 and D2R exactly as main/main-mpi.cpp:9,15 (a float constant, so the
+ * degree-to-radian product is formed in float). */
+#define ORC_PI_180 0.01745329252f
+
+/* TranslateAngleToCoefficients (main/main-mpi.cpp:85-106) followed by the
+ * linear part of DecorateCoefficients (:110-183).  The reference also carries
+ * quadratic terms a[4..9], b[4..9]; they start at zero and every decorated
+ * quadratic term is a sum of products of them, so they stay zero and the
+ * z-shift step reduces to the terms kept here. */
+void orc_coeffs(const float *angles, int nt, float offset, float pitch,
+                float zshift, double *out) {
+  const double alpha = -(pitch * ORC_PI_180), beta = offset * ORC_PI_180,
+               t = -zshift;
+  const double ca = cos(alpha), sa = sin(alpha), cb = cos(beta),
+               sb = sin(beta);
+  for (int i = 0; i < nt; ++i) {
+    /* The reference calls cos/sin on a float argument, which in C++ selects
+     * the float overloads: the angle terms carry float precision. */
+    const float tb = angles[i] * ORC_PI_180;
+    double a[4] = {0, cosf(tb), 0, -sinf(tb)};
+    double b[4] = {0, 0, 1, 0};
+    double A[4], B[4];
+    A[0] = a[0];
+    A[1] = (a[2] * sa * sb + a[3] * ca * sb + a[1] * cb);
+    A[2] = (a[2] * ca - a[3] * sa);
+    A[3] = (a[3] * ca * cb + a[2] * cb * sa - a[1] * sb);
+    B[0] = b[0];
+    B[1] = (b[2] * sa * sb + b[3] * ca * sb + b[1] * cb);
+    B[2] = (b[2] * ca - b[3] * sa);
+    B[3] = (b[3] * ca * cb + b[2] * cb * sa - b[1] * sb);
+    /* z shift (:167-182) with the quadratic terms equal to zero */
+    double *o = out + 8 * (size_t)i;
+    o[0] = A[0] + A[3] * t + 0.0 * t * t;
+    o[1] = A[1] + 0.0 * t;
+    o[2] = A[2] + 0.0 * t;
+    o[3] = A[3] + 2 * 0.0 * t;
+    o[4] = B[0] + B[3] * t + 0.0 * t * t;
+    o[5] = B[1] + 0.0 * t;
+    o[6] = B[2] + 0.0 * t;
+    o[7] = B[3] + 2 * 0.0 * t;
+  }
+}
+
+/* R-weighting filter, mode 2 (filter/filter_prj.cpp:636-736).
+ * Per row: pad from nx to N = nx + nx/10 samples with a linear ramp running
+ * from the last sample back to the first (buf2fft_padding_1D, :652-672),
+ * weight the half spectrum by W[k] (k=0: 0.2; k<=r: k; else
+ * r*exp(-(k-r)^2/sigma^2), r = floor(N*0.05f), sigma = N*0.5f; :694-723),
+ * inverse transform without normalisation, keep the first nx samples and
+ * divide by nx (:726-731).  Forward transform, weighting and unnormalised
+ * inverse together are a circular convolution of the padded row with
+ * h[d] = sum_k W_sym[k] cos(2 pi k d / N); it is evaluated here directly in
+ * double precision. */
+void orc_filter_rweight(int nx, long nrows, float *rows) {
+  const int N = nx + nx / 10;
+  const int nxp = N - nx + 1;
+  const int r = (int)floor((float)N * 0.05f);
+  const float sg = (float)N * 0.5f;
+  const int nb = N / 2 + 1;
+  double *W = (double *)malloc(sizeof(double) * nb);
+  for (int k = 0; k < nb; ++k) {
+    if (k == 0)
+      W[k] = 0.2;
+    else if (k <= r)
+      W[k] = k;
+    else
+      W[k] = (double)(float)r *
+             (double)expf(-(float)((k - r) * (k - r)) / (sg * sg));
+  }
+  double *cs = (double *)malloc(sizeof(double) * N);
+  for (int j = 0; j < N; ++j) cs[j] = cos(2.0 * 3.14159265358979323846 * j / N);
+  double *h = (double *)malloc(sizeof(double) * N);
+  const int kmax = (N % 2 == 0) ? N / 2 - 1 : (N - 1) / 2;
+  for (int d = 0; d < N; ++d) {
+    double acc = W[0];
+    for (int k = 1; k <= kmax; ++k) acc += 2.0 * W[k] * cs[(long)k * d % N];
+    if (N % 2 == 0) acc += (d % 2 == 0) ? W[N / 2] : -W[N / 2];
+    h[d] = acc;
+  }
+#pragma omp parallel
+  {
+    float *xp = (float *)malloc(sizeof(float) * N);
+#pragma omp for schedule(static)
+    for (long row = 0; row < nrows; ++row) {
+      float *x = rows + (size_t)row * nx;
+      for (int j = 0; j < nx; ++j) xp[j] = x[j];
+      for (int j = nx; j < N; ++j)
+        xp[j] = ((float)(j - nx + 1) / (float)nxp) * x[0] +
+                ((float)(N - j) / (float)nxp) * x[nx - 1];
+      for (int j = 0; j < nx; ++j) {
+        double acc = 0;
+        for (int m = 0; m < N; ++m) {
+          int d = j - m;
+          if (d < 0) d += N;
+          acc += h[d] * (double)xp[m];
+        }
+        x[j] = (float)(acc / nx);
+      }
+    }
+    free(xp);
+  }
+  free(W);
+  free(cs);
+  free(h);
+}
+
+#define PFX orc_
+#define REAL float
+#include "tiltrec_oracle_impl.h"
+#undef PFX
+#undef REAL
+
+#define PFX orc64_
+#define REAL double
+#include "tiltrec_oracle_impl.h"
+#undef PFX
+#undef REAL

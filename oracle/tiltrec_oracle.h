@@ -1,0 +1,64 @@
+/* CPU restatement of the reference TiltRec reconstruction path.
+ *
+ * TEST INFRASTRUCTURE (the oracle).  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg may load this.  It is the checker, never the
+ * product path.
+ *
+ * Parity pin: the reference ships no golden vectors or tests for TiltRec; the
+ * restatement is pinned against the unmodified reference CPU sources compiled
+ * by oracle/Makefile (`make ref`, outputs in oracle/_ref/) on seeded inputs,
+ * and the reference-generated fixtures in tests/golden/.
+ *
+ * Every function is compiled twice from tiltrec_oracle_impl.h: orc_* computes
+ * in float exactly as the reference does (double coordinates, float weights
+ * and accumulators), orc64_* replaces every float in the data path by double
+ * (the FP64 oracle used to score reduced-precision storage).
+ */
+#ifndef TILTREC_ORACLE_H
+#define TILTREC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Volume geometry.  layout 0 = Y layout (TiltRec): vol[ny][th][nx];
+ * layout 1 = Z layout (TiltRecZ): vol[th][ny][nx].  Projections are
+ * [nt][ny][nx].  z0 is the global z index of the first volume section (Z
+ * slabs); ox/oy/oz the float origin the reference passes to ValCoef. */
+typedef struct {
+  int nx, ny, nt, th;
+  int layout;
+  int z0;
+  float ox, oy, oz;
+} orc_geom;
+
+/* Per-tilt linear coefficients a0..a3, b0..b3 (main-mpi.cpp:85-183). */
+void orc_coeffs(const float *angles, int nt, float offset, float pitch,
+                float zshift, double *coeff8);
+
+/* WBP R-weighting filter, mode 2 (filter_prj.cpp:636-736), in place over
+ * nrows rows of nx floats, evaluated as a double-precision circular
+ * convolution on the padded row. */
+void orc_filter_rweight(int nx, long nrows, float *rows);
+
+#define ORC_DECLARE(PFX, REAL)                                                \
+  void PFX##backproject(const orc_geom *g, const double *coeff8,              \
+                        const REAL *proj, REAL *vol);                          \
+  void PFX##reproject(const orc_geom *g, const double *coeff8,                \
+                      const REAL *vol, REAL *val, REAL *wt);                   \
+  void PFX##update_weights(const orc_geom *g, const double *coeff8,           \
+                           const REAL *diff, REAL *valvol, REAL *wtvol);       \
+  void PFX##update_by_projdiff(const orc_geom *g, const double *coeff8,        \
+                               const REAL *diff, REAL *vol, REAL gamma);       \
+  void PFX##sirt(const orc_geom *g, const double *coeff8, const REAL *proj,   \
+                 REAL *vol, int iters, REAL gamma);                            \
+  void PFX##sart(const orc_geom *g, const double *coeff8, const REAL *proj,   \
+                 REAL *vol, int iters, REAL gamma);
+
+ORC_DECLARE(orc_, float)
+ORC_DECLARE(orc64_, double)
+
+#ifdef __cplusplus
+}
+#endif
+#endif
