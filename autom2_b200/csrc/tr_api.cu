@@ -1,0 +1,633 @@
+// C-ABI of the TiltRec B200 engine (include/tiltrec_b200.h): context,
+// geometry, scratch management and the BPT / WBP / SIRT / SART drivers.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "tiltrec_b200.h"
+#include "tr_internal.cuh"
+
+namespace trb {
+cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
+cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
+cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
+                         int nsm, cudaStream_t s);
+struct FilterArgs {
+  float *rows;
+  long long nrows;
+  int nx, n_pad;
+  int log2m;
+  const float2 *ghat;
+  const float2 *tw;
+};
+cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
+}  // namespace trb
+
+using namespace trb;
+
+namespace {
+constexpr size_t kSmemBp = 64 * 1024;  // interpolation tables per CTA
+constexpr size_t kSmemFp = 48 * 1024;  // splat windows per CTA
+constexpr size_t kSmemMax = 200 * 1024;
+}  // namespace
+
+struct tr_ctx {
+  int device = 0;
+  int nsm = 148;
+  size_t budget = 0;
+  std::string err;
+  cudaStream_t io_stream = nullptr;
+
+  // problem
+  bool have_problem = false;
+  int nx = 0, ny = 0, nt = 0, th = 0, layout = 0;
+  float ox = 0, oy = 0, oz = 0;
+  bool sep = false;
+  int fw = 0, fh = 0, chunk_bp = 1, chunk_fp = 1;
+  TiltGeo *geo_d = nullptr;
+
+  // scratch
+  size_t scratch = 0;
+  float *val_d = nullptr, *wt_d = nullptr, *wtvol_d = nullptr;
+  bool wt_ready = false, wtvol_ready = false;
+  int filt_nx = 0, filt_npad = 0, filt_log2m = 0;
+  float2 *ghat_d = nullptr, *tw_d = nullptr;
+  float *hproj_d = nullptr, *hvol_d = nullptr;
+  size_t hproj_n = 0, hvol_n = 0;
+};
+
+namespace {
+
+tr_status fail(tr_ctx *c, tr_status s, const char *fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return s;
+}
+
+tr_status cuda_fail(tr_ctx *c, cudaError_t e, const char *what) {
+  return fail(c, TR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define TR_CUDA(ctx, call)                                  \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+size_t vol_elems(const tr_ctx *c) { return (size_t)c->nx * c->ny * c->th; }
+size_t proj_elems(const tr_ctx *c) { return (size_t)c->nx * c->ny * c->nt; }
+
+tr_status scratch_alloc(tr_ctx *c, void **p, size_t bytes, const char *what) {
+  if (*p) return TR_OK;
+  if (c->budget && c->scratch + bytes > c->budget)
+    return fail(c, TR_ERR_BUDGET,
+                "%s needs %zu bytes; %zu of the %zu-byte budget in use", what,
+                bytes, c->scratch, c->budget);
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(c, TR_ERR_OOM, "cudaMalloc(%zu) for %s: %s", bytes, what,
+                cudaGetErrorString(e));
+  }
+  c->scratch += bytes;
+  return TR_OK;
+}
+
+void scratch_free(tr_ctx *c, void **p, size_t bytes) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+    c->scratch -= std::min(c->scratch, bytes);
+  }
+}
+
+void release_problem(tr_ctx *c) {
+  const size_t pb = proj_elems(c) * sizeof(float);
+  scratch_free(c, (void **)&c->val_d, pb);
+  scratch_free(c, (void **)&c->wt_d, pb);
+  scratch_free(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float));
+  if (c->geo_d) {
+    cudaFree(c->geo_d);
+    c->geo_d = nullptr;
+  }
+  c->wt_ready = c->wtvol_ready = false;
+  c->have_problem = false;
+}
+
+VolView full_view(const tr_ctx *c, float *vol, int z0, int nz) {
+  VolView v;
+  v.vol = vol;
+  v.nx = c->nx;
+  v.ny = c->ny;
+  v.nz = nz;
+  v.zoff = z0;
+  if (c->layout == TR_LAYOUT_Y) {
+    v.sy = (long long)c->th * c->nx;
+    v.sz = c->nx;
+  } else {
+    v.sy = c->nx;
+    v.sz = (long long)c->ny * c->nx;
+  }
+  return v;
+}
+
+BpArgs bp_args(const tr_ctx *c, float *vol, int z0, int nz, const float *img,
+               int t0, int nt, float gamma) {
+  BpArgs a;
+  a.v = full_view(c, vol, z0, nz);
+  a.img.p = img;
+  a.img.nx = c->nx;
+  a.img.ny = c->ny;
+  a.img.tstride = (long long)c->nx * c->ny;
+  a.geo = c->geo_d;
+  a.t0 = t0;
+  a.nt = nt;
+  a.ox = c->ox;
+  a.oy = c->oy;
+  a.oz = c->oz;
+  a.fw = c->fw;
+  a.fh = c->fh;
+  a.chunk = c->chunk_bp;
+  a.gamma = gamma;
+  a.wtvol = nullptr;
+  a.out = nullptr;
+  return a;
+}
+
+FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
+               int t0, int nt) {
+  FpArgs a;
+  a.v = full_view(c, const_cast<float *>(vol), z0, nz);
+  a.val = val;
+  a.tstride = (long long)c->nx * c->ny;
+  a.pnx = c->nx;
+  a.pny = c->ny;
+  a.geo = c->geo_d;
+  a.t0 = t0;
+  a.nt = nt;
+  a.ox = c->ox;
+  a.oy = c->oy;
+  a.oz = c->oz;
+  a.fw = c->fw;
+  a.fh = c->fh;
+  a.chunk = c->chunk_fp;
+  return a;
+}
+
+// Iterative radix-2 FFT in double (host), forward sign -1.
+void fft_host(std::vector<std::complex<double>> &x) {
+  const size_t n = x.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(x[i], x[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    const double ang = -2.0 * M_PI / (double)len;
+    for (size_t i = 0; i < n; i += len)
+      for (size_t k = 0; k < len / 2; ++k) {
+        const std::complex<double> w(cos(ang * k), sin(ang * k));
+        const std::complex<double> u = x[i + k], v = x[i + k + len / 2] * w;
+        x[i + k] = u + v;
+        x[i + k + len / 2] = u - v;
+      }
+  }
+}
+
+// Kernel spectrum of the R-weighting filter for rows of nx samples.
+tr_status build_filter(tr_ctx *c, int nx) {
+  if (c->filt_nx == nx && c->ghat_d) return TR_OK;
+  const int N = nx + nx / 10;
+  int log2m = 1;
+  while ((1 << log2m) < N + nx - 1) ++log2m;
+  const int M = 1 << log2m;
+  if ((size_t)M * sizeof(float2) > kSmemMax)
+    return fail(c, TR_ERR_UNSUPPORTED, "row length %d needs an FFT of %d points", nx, M);
+  // Weights exactly as filter_prj.cpp:694-723 forms them (float arithmetic).
+  const int r = (int)floor((float)N * 0.05f);
+  const float sg = (float)N * 0.5f;
+  const int nb = N / 2 + 1;
+  std::vector<double> W(nb);
+  for (int k = 0; k < nb; ++k) {
+    if (k == 0)
+      W[k] = 0.2;
+    else if (k <= r)
+      W[k] = k;
+    else
+      W[k] = (double)(float)r * (double)expf(-(float)((k - r) * (k - r)) / (sg * sg));
+  }
+  // h[d] = sum over the Hermitian-extended spectrum of W cos(2 pi k d / N).
+  std::vector<double> cs(N), h(N);
+  for (int j = 0; j < N; ++j) cs[j] = cos(2.0 * M_PI * j / N);
+  const int kmax = (N % 2 == 0) ? N / 2 - 1 : (N - 1) / 2;
+  for (int d = 0; d < N; ++d) {
+    double acc = W[0];
+    for (int k = 1; k <= kmax; ++k) acc += 2.0 * W[k] * cs[(long long)k * d % N];
+    if (N % 2 == 0) acc += (d % 2 == 0) ? W[N / 2] : -W[N / 2];
+    h[d] = acc;
+  }
+  std::vector<std::complex<double>> g(M, 0.0);
+  for (int e = -(N - 1); e <= nx - 1; ++e) g[(e % M + M) % M] = h[(e % N + N) % N];
+  fft_host(g);
+  std::vector<float2> ghat(M), tw(M / 2);
+  const double scale = 1.0 / ((double)M * nx);
+  for (int i = 0; i < M; ++i) {
+    int br = 0;
+    for (int b = 0; b < log2m; ++b) br |= ((i >> b) & 1) << (log2m - 1 - b);
+    ghat[i] = make_float2((float)(g[br].real() * scale), (float)(g[br].imag() * scale));
+  }
+  for (int k = 0; k < M / 2; ++k)
+    tw[k] = make_float2((float)cos(2.0 * M_PI * k / M), (float)-sin(2.0 * M_PI * k / M));
+  if (c->ghat_d) scratch_free(c, (void **)&c->ghat_d, sizeof(float2) << c->filt_log2m);
+  if (c->tw_d) scratch_free(c, (void **)&c->tw_d, sizeof(float2) << (c->filt_log2m - 1));
+  tr_status s = scratch_alloc(c, (void **)&c->ghat_d, sizeof(float2) * M, "filter spectrum");
+  if (s) return s;
+  s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * (M / 2), "filter twiddles");
+  if (s) return s;
+  TR_CUDA(c, cudaMemcpy(c->ghat_d, ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+  TR_CUDA(c, cudaMemcpy(c->tw_d, tw.data(), sizeof(float2) * (M / 2), cudaMemcpyHostToDevice));
+  c->filt_nx = nx;
+  c->filt_npad = N;
+  c->filt_log2m = log2m;
+  return TR_OK;
+}
+
+// Validates coefficients, derives the fixed-point steps and the per-tile
+// detector window, and uploads them (ordered on `s`).  Invalidates the cached
+// SIRT/SART weights, which depend on the geometry.
+tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
+  const int nt = c->nt;
+  std::vector<TiltGeo> g(nt);
+  bool sep = true;
+  double span_u = 0, span_v = 0;
+  const double two32 = 4294967296.0;
+  const double ext = std::max(std::max(c->nx, c->ny), c->th) + 64.0;
+  for (int t = 0; t < nt; ++t) {
+    const double *k = coeff8 + 8 * (size_t)t;
+    for (int i = 0; i < 4; ++i) {
+      g[t].a[i] = k[i];
+      g[t].b[i] = k[4 + i];
+      if (!std::isfinite(k[i]) || !std::isfinite(k[4 + i]))
+        return fail(c, TR_ERR_ARG, "non-finite coefficient at tilt %d", t);
+    }
+    for (int i = 0; i < 3; ++i) {
+      if (fabs(k[1 + i]) > 1024.0 || fabs(k[5 + i]) > 1024.0)
+        return fail(c, TR_ERR_UNSUPPORTED, "coefficient magnitude above 1024 at tilt %d", t);
+      g[t].A[i] = llrint(k[1 + i] * two32);
+      g[t].B[i] = llrint(k[5 + i] * two32);
+    }
+    // Detector coordinates must stay far inside the int range of the table
+    // origins for every voxel of the volume.
+    const double reach_u = fabs(k[0]) + (fabs(k[1]) + fabs(k[2]) + fabs(k[3])) * 2 * ext;
+    const double reach_v = fabs(k[4]) + (fabs(k[5]) + fabs(k[6]) + fabs(k[7])) * 2 * ext;
+    if (reach_u > 1.0e9 || reach_v > 1.0e9)
+      return fail(c, TR_ERR_UNSUPPORTED, "detector coordinates out of range at tilt %d", t);
+    if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
+    span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
+                                  fabs(k[3]) * (kTZ - 1));
+    span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
+                                  fabs(k[7]) * (kTZ - 1));
+  }
+  const int fw = (int)ceil(span_u) + 4;
+  const int fh = sep ? kTY : (int)ceil(span_v) + 5;
+  const size_t ent_bp = (size_t)fw * fh * sizeof(float2);
+  const size_t ent_fp = (size_t)fw * fh * sizeof(float);
+  if (ent_bp > kSmemMax)
+    return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds shared memory",
+                fw, fh);
+  if (s) {
+    TR_CUDA(c, cudaMemcpyAsync(c->geo_d, g.data(), sizeof(TiltGeo) * nt,
+                               cudaMemcpyHostToDevice, s));
+    TR_CUDA(c, cudaStreamSynchronize(s));
+  } else {
+    TR_CUDA(c, cudaMemcpy(c->geo_d, g.data(), sizeof(TiltGeo) * nt, cudaMemcpyHostToDevice));
+  }
+  c->fw = fw;
+  c->fh = fh;
+  c->sep = sep;
+  c->chunk_bp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemBp / ent_bp));
+  c->chunk_fp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemFp / ent_fp));
+  c->wt_ready = c->wtvol_ready = false;
+  return TR_OK;
+}
+
+tr_status need_problem(tr_ctx *c) {
+  if (!c) return TR_ERR_ARG;
+  if (!c->have_problem) return fail(c, TR_ERR_NOPROBLEM, "tr_set_problem has not been called");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+  return TR_OK;
+}
+
+tr_status ensure_wt(tr_ctx *c, cudaStream_t s) {
+  const size_t pb = proj_elems(c) * sizeof(float);
+  tr_status st = scratch_alloc(c, (void **)&c->wt_d, pb, "projection weights");
+  if (st) return st;
+  if (!c->wt_ready) {
+    TR_CUDA(c, cudaMemsetAsync(c->wt_d, 0, pb, s));
+    FpArgs a = fp_args(c, nullptr, 0, c->th, c->wt_d, 0, c->nt);
+    TR_CUDA(c, launch_fp(c->sep, a, s));
+    c->wt_ready = true;
+  }
+  return TR_OK;
+}
+
+tr_status ensure_wtvol(tr_ctx *c, cudaStream_t s) {
+  tr_status st = scratch_alloc(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float),
+                               "voxel weights");
+  if (st) return st;
+  if (!c->wtvol_ready) {
+    BpArgs a = bp_args(c, c->wtvol_d, 0, c->th, nullptr, 0, c->nt, 1.f);
+    a.out = c->wtvol_d;
+    TR_CUDA(c, launch_bp(BP_WEIGHTS, c->sep, a, s));
+    c->wtvol_ready = true;
+  }
+  return TR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tr_version(void) { return 10000; }
+
+const char *tr_status_string(int s) {
+  switch (s) {
+    case TR_OK: return "ok";
+    case TR_ERR_ARG: return "invalid argument";
+    case TR_ERR_OOM: return "device out of memory";
+    case TR_ERR_BUDGET: return "HBM budget exceeded";
+    case TR_ERR_CUDA: return "CUDA error";
+    case TR_ERR_TIMEOUT: return "device wait timed out";
+    case TR_ERR_NOPROBLEM: return "no problem set";
+    case TR_ERR_UNSUPPORTED: return "unsupported geometry";
+    default: return "unknown status";
+  }
+}
+
+tr_status tr_geometry_from_angles(const float *angles, int nt, float offset,
+                                  float pitch, float zshift, double *out) {
+  if (!angles || !out || nt <= 0) return TR_ERR_ARG;
+  // D2R with the reference's float constant (main-mpi.cpp:9,15): the
+  // product is formed in float.  cos/sin of a float angle resolve to the
+  // float overloads in the reference's C++ (TranslateAngleToCoefficients,
+  // :94-98), of the double alpha/beta to the double ones (:112-113).
+  const float kPi180 = 0.01745329252f;
+  const double alpha = -(pitch * kPi180), beta = offset * kPi180, t = -zshift;
+  const double ca = cos(alpha), sa = sin(alpha), cb = cos(beta), sb = sin(beta);
+  for (int i = 0; i < nt; ++i) {
+    const float tb = angles[i] * kPi180;
+    const double a1 = cosf(tb), a3 = -sinf(tb);
+    // DecorateCoefficients (:121-146) with a = (0, a1, 0, a3), b = (0, 0, 1, 0),
+    // then the z shift (:173-181); the quadratic terms are all zero.
+    const double A1 = 0.0 * sa * sb + a3 * ca * sb + a1 * cb;
+    const double A2 = 0.0 * ca - a3 * sa;
+    const double A3 = a3 * ca * cb + 0.0 * cb * sa - a1 * sb;
+    const double B1 = 1.0 * sa * sb + 0.0 * ca * sb + 0.0 * cb;
+    const double B2 = 1.0 * ca - 0.0 * sa;
+    const double B3 = 0.0 * ca * cb + 1.0 * cb * sa - 0.0 * sb;
+    double *o = out + 8 * (size_t)i;
+    o[0] = 0.0 + A3 * t + 0.0 * t * t;
+    o[1] = A1 + 0.0 * t;
+    o[2] = A2 + 0.0 * t;
+    o[3] = A3 + 2 * 0.0 * t;
+    o[4] = 0.0 + B3 * t + 0.0 * t * t;
+    o[5] = B1 + 0.0 * t;
+    o[6] = B2 + 0.0 * t;
+    o[7] = B3 + 2 * 0.0 * t;
+  }
+  return TR_OK;
+}
+
+tr_status tr_create(int device, size_t budget, tr_ctx **out) {
+  if (!out) return TR_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return TR_ERR_ARG;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return TR_ERR_CUDA;
+  tr_ctx *c = new tr_ctx;
+  c->device = device;
+  c->budget = budget;
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->io_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return TR_ERR_CUDA;
+  }
+  *out = c;
+  return TR_OK;
+}
+
+tr_status tr_destroy(tr_ctx *c) {
+  if (!c) return TR_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaDeviceSynchronize();
+  release_problem(c);
+  scratch_free(c, (void **)&c->ghat_d, 0);
+  scratch_free(c, (void **)&c->tw_d, 0);
+  if (c->hproj_d) cudaFree(c->hproj_d);
+  if (c->hvol_d) cudaFree(c->hvol_d);
+  if (c->io_stream) cudaStreamDestroy(c->io_stream);
+  delete c;
+  return TR_OK;
+}
+
+const char *tr_last_error(const tr_ctx *c) { return c ? c->err.c_str() : "null context"; }
+size_t tr_scratch_bytes(const tr_ctx *c) { return c ? c->scratch : 0; }
+
+tr_status tr_set_problem(tr_ctx *c, int nx, int ny, int nt, int th, int layout,
+                         const double *coeff8, float ox, float oy, float oz) {
+  if (!c) return TR_ERR_ARG;
+  if (nx < 2 || ny < 1 || nt < 1 || th < 1 || !coeff8 ||
+      (layout != TR_LAYOUT_Y && layout != TR_LAYOUT_Z))
+    return fail(c, TR_ERR_ARG, "bad problem: nx=%d ny=%d ntilt=%d th=%d layout=%d",
+                nx, ny, nt, th, layout);
+  if ((double)nx * ny * th > 9.0e18 || ny > 65535 * kTY)
+    return fail(c, TR_ERR_ARG, "problem too large");
+  TR_CUDA(c, cudaSetDevice(c->device));
+  TR_CUDA(c, cudaDeviceSynchronize());
+  release_problem(c);
+  c->nx = nx;
+  c->ny = ny;
+  c->nt = nt;
+  c->th = th;
+  TR_CUDA(c, cudaMalloc(&c->geo_d, sizeof(TiltGeo) * nt));
+  tr_status st = load_geometry(c, coeff8, nullptr);
+  if (st) {
+    cudaFree(c->geo_d);
+    c->geo_d = nullptr;
+    return st;
+  }
+  c->layout = layout;
+  c->ox = ox;
+  c->oy = oy;
+  c->oz = oz;
+  c->have_problem = true;
+  return TR_OK;
+}
+
+tr_status tr_update_geometry(tr_ctx *c, const double *coeff8, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!coeff8) return fail(c, TR_ERR_ARG, "null coefficients");
+  // The old geometry may still be in use by queued kernels on `stream`.
+  return load_geometry(c, coeff8, stream ? (cudaStream_t)stream : c->io_stream);
+}
+
+tr_status tr_filter_rweight(tr_ctx *c, float *proj, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj) return fail(c, TR_ERR_ARG, "null projections");
+  st = build_filter(c, c->nx);
+  if (st) return st;
+  FilterArgs f;
+  f.rows = proj;
+  f.nrows = (long long)c->ny * c->nt;
+  f.nx = c->nx;
+  f.n_pad = c->filt_npad;
+  f.log2m = c->filt_log2m;
+  f.ghat = c->ghat_d;
+  f.tw = c->tw_d;
+  TR_CUDA(c, launch_rweight(f, (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_backproject(tr_ctx *c, const float *proj, float *vol, int z0, int nz,
+                         void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || z0 < 0 || nz < 1 || z0 + nz > c->th)
+    return fail(c, TR_ERR_ARG, "bad back-projection arguments (z0=%d nz=%d)", z0, nz);
+  BpArgs a = bp_args(c, vol, z0, nz, proj, 0, c->nt, 1.f);
+  TR_CUDA(c, launch_bp(BP_NORM, c->sep, a, (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_forward_project(tr_ctx *c, const float *vol, int z0, int nz, float *val,
+                             float *wt, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!vol || !val || z0 < 0 || nz < 1 || z0 + nz > c->th)
+    return fail(c, TR_ERR_ARG, "bad forward-projection arguments (z0=%d nz=%d)", z0, nz);
+  FpArgs a = fp_args(c, vol, z0, nz, val, 0, c->nt);
+  TR_CUDA(c, launch_fp(c->sep, a, (cudaStream_t)stream));
+  if (wt) {
+    FpArgs w = fp_args(c, nullptr, z0, nz, wt, 0, c->nt);
+    TR_CUDA(c, launch_fp(c->sep, w, (cudaStream_t)stream));
+  }
+  return TR_OK;
+}
+
+tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gamma,
+                  void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || iters < 0) return fail(c, TR_ERR_ARG, "bad SIRT arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t pn = proj_elems(c);
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection"))) return st;
+  if ((st = ensure_wt(c, s))) return st;
+  if ((st = ensure_wtvol(c, s))) return st;
+  for (int it = 0; it < iters; ++it) {
+    TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
+    FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
+    TR_CUDA(c, launch_fp(c->sep, f, s));
+    TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
+    BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, 0, c->nt, gamma);
+    b.wtvol = c->wtvol_d;
+    TR_CUDA(c, launch_bp(BP_SIRT, c->sep, b, s));
+  }
+  return TR_OK;
+}
+
+tr_status tr_sart(tr_ctx *c, const float *proj, float *vol, int iters, float gamma,
+                  void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || iters < 0) return fail(c, TR_ERR_ARG, "bad SART arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t plane = (size_t)c->nx * c->ny;
+  if ((st = scratch_alloc(c, (void **)&c->val_d, proj_elems(c) * sizeof(float),
+                          "reprojection")))
+    return st;
+  if ((st = ensure_wt(c, s))) return st;
+  for (int it = 0; it < iters; ++it)
+    for (int t = 0; t < c->nt; ++t) {
+      float *vt = c->val_d + plane * t;
+      TR_CUDA(c, cudaMemsetAsync(vt, 0, plane * sizeof(float), s));
+      FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, t, 1);
+      TR_CUDA(c, launch_fp(c->sep, f, s));
+      TR_CUDA(c, launch_resid(proj + plane * t, vt, c->wt_d + plane * t, plane, c->nsm, s));
+      BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, t, 1, gamma);
+      TR_CUDA(c, launch_bp(BP_NORM, c->sep, b, s));
+    }
+  return TR_OK;
+}
+
+tr_status tr_wbp(tr_ctx *c, float *proj, float *vol, void *stream) {
+  tr_status st = tr_filter_rweight(c, proj, stream);
+  if (st) return st;
+  return tr_backproject(c, proj, vol, 0, c->th, stream);
+}
+
+tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float *vol_h,
+                              int iters, float gamma) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
+  const size_t pn = proj_elems(c), vn = vol_elems(c);
+  if (c->hproj_n != pn) {
+    if (c->hproj_d) cudaFree(c->hproj_d);
+    c->hproj_d = nullptr;
+    c->hproj_n = 0;
+    TR_CUDA(c, cudaMalloc(&c->hproj_d, pn * sizeof(float)));
+    c->hproj_n = pn;
+  }
+  if (c->hvol_n != vn) {
+    if (c->hvol_d) cudaFree(c->hvol_d);
+    c->hvol_d = nullptr;
+    c->hvol_n = 0;
+    TR_CUDA(c, cudaMalloc(&c->hvol_d, vn * sizeof(float)));
+    c->hvol_n = vn;
+  }
+  cudaStream_t s = c->io_stream;
+  TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice, s));
+  TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));
+  switch (method) {
+    case TR_METHOD_BPT: st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s); break;
+    case TR_METHOD_WBP: st = tr_wbp(c, c->hproj_d, c->hvol_d, s); break;
+    case TR_METHOD_SIRT: st = tr_sirt(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
+    case TR_METHOD_SART: st = tr_sart(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
+    default: st = fail(c, TR_ERR_ARG, "unknown method %d", method);
+  }
+  if (st) return st;
+  TR_CUDA(c, cudaMemcpyAsync(vol_h, c->hvol_d, vn * sizeof(float), cudaMemcpyDeviceToHost, s));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  return TR_OK;
+}
+
+tr_status tr_synchronize(tr_ctx *c) {
+  if (!c) return TR_ERR_ARG;
+  TR_CUDA(c, cudaSetDevice(c->device));
+  TR_CUDA(c, cudaDeviceSynchronize());
+  return TR_OK;
+}
+
+}  // extern "C"

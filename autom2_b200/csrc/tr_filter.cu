@@ -1,0 +1,117 @@
+// WBP R-weighting filter (filter/filter_prj.cpp:636-736, ApplyFilterInplace
+// mode 2, :787-795) as one shared-memory FFT convolution per pair of rows.
+//
+// The reference pads each row of nx samples to N = nx + nx/10 with a linear
+// ramp from the last sample back to the first, takes a real FFT of length N,
+// scales bin k by W[k] (0.2 at k = 0, k up to r = floor(0.05 N), then a
+// Gaussian roll-off r exp(-(k-r)^2 / (N/2)^2)), inverse transforms without
+// normalisation, keeps the first nx samples and divides by nx.  That whole
+// chain is a circular convolution of the padded row with a fixed real kernel
+// h (length N).  N is generally not a power of two (281, 1126, 2252, 4505 for
+// nx = 256..4096), so the circular convolution is evaluated as a linear one on
+// a power-of-two length M >= N + nx - 1 with the kernel laid out for
+// lags -(N-1)..nx-1; no wrap-around reaches the kept outputs.  The kernel's
+// spectrum (already scaled by 1/(M nx) and permuted to bit-reversed order) is
+// built once on the host in double precision.
+//
+// Per CTA: rows r and r+1 become the real and imaginary parts of one complex
+// sequence in shared memory; a radix-2 decimation-in-frequency pass sequence
+// (natural in, bit-reversed out), a pointwise product with the spectrum, and a
+// decimation-in-time inverse (bit-reversed in, natural out) give both filtered
+// rows at once because the kernel is real.
+#include <cuda_runtime.h>
+
+namespace trb {
+
+struct FilterArgs {
+  float *rows;          // [nrows][nx], filtered in place
+  long long nrows;
+  int nx, n_pad;        // row length and the reference's padded length N
+  int log2m;            // M = 1 << log2m
+  const float2 *ghat;   // [M] kernel spectrum, bit-reversed, scaled
+  const float2 *tw;     // [M/2] e^{-2 pi i k / M}
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+__global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
+  extern __shared__ float2 buf[];
+  const int M = 1 << f.log2m, half = M >> 1;
+  const long long r0 = 2ll * blockIdx.x;
+  const bool has1 = r0 + 1 < f.nrows;
+  const float *x0 = f.rows + r0 * f.nx;
+  const float *x1 = has1 ? x0 + f.nx : nullptr;
+  const int nx = f.nx, N = f.n_pad;
+  const int nxp = N - nx + 1;
+  const float a0 = x0[0], b0 = x0[nx - 1];
+  const float a1 = has1 ? x1[0] : 0.f, b1 = has1 ? x1[nx - 1] : 0.f;
+
+  // Padded rows (buf2fft_padding_1D, filter_prj.cpp:652-672), zero beyond N.
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    float re = 0.f, im = 0.f;
+    if (j < nx) {
+      re = x0[j];
+      im = has1 ? x1[j] : 0.f;
+    } else if (j < N) {
+      const float wa = (float)(j - nx + 1) / (float)nxp;
+      const float wb = (float)(N - j) / (float)nxp;
+      re = wa * a0 + wb * b0;
+      im = wa * a1 + wb * b1;
+    }
+    buf[j] = make_float2(re, im);
+  }
+  __syncthreads();
+
+  // Forward DIF.
+  for (int h = half, ts = 1; h >= 1; h >>= 1, ts <<= 1) {
+    for (int b = threadIdx.x; b < half; b += blockDim.x) {
+      const int grp = b / h, pos = b - grp * h;
+      const int i0 = grp * 2 * h + pos, i1 = i0 + h;
+      const float2 u = buf[i0], v = buf[i1];
+      buf[i0] = make_float2(u.x + v.x, u.y + v.y);
+      buf[i1] = cmul(make_float2(u.x - v.x, u.y - v.y), __ldg(f.tw + pos * ts));
+    }
+    __syncthreads();
+  }
+  // Spectrum product (both in bit-reversed order).
+  for (int j = threadIdx.x; j < M; j += blockDim.x)
+    buf[j] = cmul(buf[j], __ldg(f.ghat + j));
+  __syncthreads();
+  // Inverse DIT.
+  for (int h = 1, ts = half; h < M; h <<= 1, ts >>= 1) {
+    for (int b = threadIdx.x; b < half; b += blockDim.x) {
+      const int grp = b / h, pos = b - grp * h;
+      const int i0 = grp * 2 * h + pos, i1 = i0 + h;
+      const float2 u = buf[i0];
+      const float2 v = cmulc(buf[i1], __ldg(f.tw + pos * ts));
+      buf[i0] = make_float2(u.x + v.x, u.y + v.y);
+      buf[i1] = make_float2(u.x - v.x, u.y - v.y);
+    }
+    __syncthreads();
+  }
+  float *y0 = f.rows + r0 * f.nx;
+  for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+    const float2 z = buf[j];
+    y0[j] = z.x;
+    if (has1) y0[f.nx + j] = z.y;
+  }
+}
+
+cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s) {
+  const int M = 1 << f.log2m;
+  const size_t smem = (size_t)M * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(
+      rweight_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long pairs = (f.nrows + 1) / 2;
+  const int threads = M >= 8192 ? 512 : 256;
+  rweight_kernel<<<(unsigned)pairs, threads, smem, s>>>(f);
+  return cudaGetLastError();
+}
+
+}  // namespace trb

@@ -1,0 +1,227 @@
+"""Python host binding of the TiltRec B200 engine (ctypes over the C ABI in
+``include/tiltrec_b200.h``).
+
+It mirrors the reference's reconstruction interface for this path:
+
+==========================  ==================================================
+reference                   here
+==========================  ==================================================
+TranslateAngleToCoefficients + DecorateCoefficients
+  (main/main-mpi.cpp:85-183)  :func:`geometry_from_angles`
+ApplyFilterInplace mode 2    :meth:`Engine.filter_rweight`
+  (filter/filter_prj.cpp:738)
+BackProject                  :meth:`Engine.backproject`
+  (main-mpi.cpp:411; main-mpiz.cpp:322)
+Reproject                    :meth:`Engine.forward_project`
+  (main-mpi.cpp:286; main-mpiz.cpp:197)
+SIRT / SART                  :meth:`Engine.sirt` / :meth:`Engine.sart`
+  (main-mpi.cpp:614 / :578)
+WBP (filter + BackProject)   :meth:`Engine.wbp` (main-mpi.cpp:841-846)
+==========================  ==================================================
+
+Device arrays are torch CUDA tensors (float32, contiguous); torch supplies
+memory and streams only, all arithmetic runs in the library's sm_100a kernels.
+There is no CPU fallback: constructing an :class:`Engine` without the built
+library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+LAYOUT_Y, LAYOUT_Z = 0, 1
+METHOD_BPT, METHOD_WBP, METHOD_SIRT, METHOD_SART = 0, 1, 2, 3
+METHODS = {"BPT": METHOD_BPT, "WBP": METHOD_WBP, "SIRT": METHOD_SIRT,
+           "SART": METHOD_SART}
+
+_lib = None
+
+
+class TiltRecError(RuntimeError):
+    """A C-ABI call returned a non-zero tr_status."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"tr_status {status}: {message}")
+        self.status = status
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Load ``libtiltrec_b200.so``; raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    path = path or library_path()
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m autom2_b200.build`")
+    lib = C.CDLL(path)
+    vp, i, f, d, sz = C.c_void_p, C.c_int, C.c_float, C.c_double, C.c_size_t
+    dp = C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
+    lib.tr_version.restype = i
+    lib.tr_status_string.argtypes = [i]
+    lib.tr_status_string.restype = C.c_char_p
+    lib.tr_geometry_from_angles.argtypes = [fp, i, f, f, f, dp]
+    lib.tr_create.argtypes = [i, sz, C.POINTER(vp)]
+    lib.tr_destroy.argtypes = [vp]
+    lib.tr_last_error.argtypes = [vp]
+    lib.tr_last_error.restype = C.c_char_p
+    lib.tr_scratch_bytes.argtypes = [vp]
+    lib.tr_scratch_bytes.restype = sz
+    lib.tr_set_problem.argtypes = [vp, i, i, i, i, i, dp, f, f, f]
+    lib.tr_update_geometry.argtypes = [vp, dp, vp]
+    lib.tr_filter_rweight.argtypes = [vp, vp, vp]
+    lib.tr_backproject.argtypes = [vp, vp, vp, i, i, vp]
+    lib.tr_forward_project.argtypes = [vp, vp, i, i, vp, vp, vp]
+    lib.tr_sirt.argtypes = [vp, vp, vp, i, f, vp]
+    lib.tr_sart.argtypes = [vp, vp, vp, i, f, vp]
+    lib.tr_wbp.argtypes = [vp, vp, vp, vp]
+    lib.tr_reconstruct_host.argtypes = [vp, i, vp, vp, i, f]
+    lib.tr_synchronize.argtypes = [vp]
+    for name in ("tr_create", "tr_destroy", "tr_set_problem", "tr_update_geometry",
+                 "tr_filter_rweight",
+                 "tr_backproject", "tr_forward_project", "tr_sirt", "tr_sart",
+                 "tr_wbp", "tr_reconstruct_host", "tr_synchronize",
+                 "tr_geometry_from_angles"):
+        getattr(lib, name).restype = i
+    if path == library_path():
+        _lib = lib
+    return lib
+
+
+def geometry_from_angles(angles, offset=0.0, pitch=0.0, zshift=0.0) -> np.ndarray:
+    """Per-tilt coefficients [ntilt][8] (a0..a3, b0..b3), bit-identical to the
+    reference's TranslateAngleToCoefficients + DecorateCoefficients."""
+    lib = load_library()
+    a = np.ascontiguousarray(angles, np.float32)
+    out = np.zeros((a.size, 8), np.float64)
+    st = lib.tr_geometry_from_angles(a.ctypes.data_as(C.POINTER(C.c_float)), a.size,
+                                     float(offset), float(pitch), float(zshift),
+                                     out.ctypes.data_as(C.POINTER(C.c_double)))
+    if st:
+        raise TiltRecError(st, "tr_geometry_from_angles")
+    return out
+
+
+def default_origin(layout: int, nx: int, ny: int, th: int):
+    """The float origin the reference CLIs use: TiltRec-mpi (Y layout) takes
+    (nx/2, th/2, th/2) (main-mpi.cpp:743-745, mrcvol.Y() is the thickness);
+    TiltRecZ (Z layout) takes (nx/2, ny/2, th/2) (main-mpiz.cpp:1078-1080)."""
+    if layout == LAYOUT_Y:
+        return (nx * 0.5, th * 0.5, th * 0.5)
+    return (nx * 0.5, ny * 0.5, th * 0.5)
+
+
+def _ptr(t) -> int:
+    return t.data_ptr() if t is not None else 0
+
+
+def _stream(device: int):
+    import torch
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Engine:
+    """One C-ABI context (``tr_ctx``) bound to a CUDA device."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        self.lib = load_library()
+        self.device = device
+        h = C.c_void_p()
+        st = self.lib.tr_create(device, hbm_budget, C.byref(h))
+        if st:
+            raise TiltRecError(st, f"tr_create(device={device}) failed "
+                                   f"({self.lib.tr_status_string(st).decode()})")
+        self.h = h
+        self.shape = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, what: str):
+        if st:
+            msg = self.lib.tr_last_error(self.h).decode()
+            raise TiltRecError(st, f"{what}: {msg}")
+
+    @property
+    def scratch_bytes(self) -> int:
+        return int(self.lib.tr_scratch_bytes(self.h))
+
+    def set_problem(self, nx, ny, ntilt, thickness, coeff8, layout=LAYOUT_Y,
+                    origin=None):
+        c = np.ascontiguousarray(coeff8, np.float64).reshape(ntilt, 8)
+        ox, oy, oz = origin if origin is not None else default_origin(layout, nx, ny, thickness)
+        self._check(self.lib.tr_set_problem(self.h, nx, ny, ntilt, thickness, layout,
+                                            c.ctypes.data_as(C.POINTER(C.c_double)),
+                                            ox, oy, oz), "tr_set_problem")
+        self.shape = (nx, ny, ntilt, thickness, layout)
+
+    def update_geometry(self, coeff8):
+        nt = self.shape[2]
+        c = np.ascontiguousarray(coeff8, np.float64).reshape(nt, 8)
+        self._check(self.lib.tr_update_geometry(self.h, c.ctypes.data_as(C.POINTER(C.c_double)),
+                                                _stream(self.device)), "tr_update_geometry")
+
+    def vol_shape(self):
+        nx, ny, nt, th, layout = self.shape
+        return (ny, th, nx) if layout == LAYOUT_Y else (th, ny, nx)
+
+    def proj_shape(self):
+        nx, ny, nt, th, _ = self.shape
+        return (nt, ny, nx)
+
+    def filter_rweight(self, proj):
+        self._check(self.lib.tr_filter_rweight(self.h, _ptr(proj), _stream(self.device)),
+                    "tr_filter_rweight")
+
+    def backproject(self, proj, vol, z0=0, nz=None):
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_backproject(self.h, _ptr(proj), _ptr(vol), z0, nz,
+                                            _stream(self.device)), "tr_backproject")
+
+    def forward_project(self, vol, val, wt=None, z0=0, nz=None):
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_forward_project(self.h, _ptr(vol), z0, nz, _ptr(val),
+                                                _ptr(wt), _stream(self.device)),
+                    "tr_forward_project")
+
+    def sirt(self, proj, vol, iters, gamma):
+        self._check(self.lib.tr_sirt(self.h, _ptr(proj), _ptr(vol), iters, gamma,
+                                     _stream(self.device)), "tr_sirt")
+
+    def sart(self, proj, vol, iters, gamma):
+        self._check(self.lib.tr_sart(self.h, _ptr(proj), _ptr(vol), iters, gamma,
+                                     _stream(self.device)), "tr_sart")
+
+    def wbp(self, proj, vol):
+        self._check(self.lib.tr_wbp(self.h, _ptr(proj), _ptr(vol), _stream(self.device)),
+                    "tr_wbp")
+
+    def reconstruct_host(self, method, proj: np.ndarray, vol: np.ndarray, iters=0,
+                         gamma=0.0):
+        """Host buffers in, host volume out (vol is updated in place)."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        assert proj.dtype == np.float32 and proj.flags.c_contiguous
+        assert vol.dtype == np.float32 and vol.flags.c_contiguous
+        self._check(self.lib.tr_reconstruct_host(self.h, m, proj.ctypes.data,
+                                                 vol.ctypes.data, iters, gamma),
+                    "tr_reconstruct_host")
+
+    def synchronize(self):
+        self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")

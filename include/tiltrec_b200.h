@@ -1,0 +1,155 @@
+/* tiltrec_b200 -- C ABI of the B200 (sm_100a) TiltRec reconstruction engine.
+ *
+ * Drop-in boundary for the reference's reconstruction drivers.  The reference
+ * binds its hot path as C++ calls that own device memory and write MRC files
+ * (src/TiltRec/src/TiltRec_cuda_y/recon_y.cuh:25-40,
+ *  src/TiltRec/src/TiltRec_cuda_z/recon_z.cuh:17-39) and as CPU routines in
+ * src/TiltRec/src/main/main-mpi.cpp / main-mpiz.cpp.  This ABI exposes the
+ * same operations on caller-owned buffers: plain pointers and sizes, no C++ or
+ * CUDA types (streams are passed as void*, i.e. a cudaStream_t or NULL for
+ * the legacy default stream).
+ *
+ * Data layout (all float32, C order):
+ *   projections  [ntilt][ny][nx]            (MRC stack X, Y, Z = tilts)
+ *   volume, Y    [ny][thickness][nx]        (TiltRec:  MRC (X, th, Y))
+ *   volume, Z    [thickness][ny][nx]        (TiltRecZ: MRC (X, Y, th))
+ *   coefficients [ntilt][8] double          a0 a1 a2 a3 b0 b1 b2 b3: a voxel
+ *       at (x, y, z) projects to detector column
+ *       u = a0 + a1 (x-ox) + a2 (y-oy) + a3 (z-oz) + ox and row
+ *       v = b0 + b1 (x-ox) + b2 (y-oy) + b3 (z-oz) + oy
+ *       (the linear part of the reference's struct Coeff, main-mpi.cpp:19-30,
+ *       as evaluated by ValCoef, main-mpi.cpp:204-226).
+ *
+ * Conventions: every call returns a tr_status (0 = OK, negative = error; the
+ * message is in tr_last_error).  No call exits the process.  Device calls are
+ * asynchronous and ordered on the given stream.  A context is not safe for
+ * concurrent use by several host threads; use one context per thread/stream.
+ * The library owns only scratch memory, allocated within the context's HBM
+ * budget (0 = unlimited). */
+#ifndef TILTREC_B200_H
+#define TILTREC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Every declaration below is an exported symbol of libtiltrec_b200.so (the
+ * library is built with hidden visibility by default). */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct tr_ctx tr_ctx;
+
+typedef enum {
+  TR_OK = 0,
+  TR_ERR_ARG = -1,         /* invalid argument / state for this call */
+  TR_ERR_OOM = -2,         /* device allocation failed */
+  TR_ERR_BUDGET = -3,      /* scratch would exceed the HBM budget */
+  TR_ERR_CUDA = -4,        /* CUDA runtime error (see tr_last_error) */
+  TR_ERR_TIMEOUT = -5,     /* a bounded device wait ran out */
+  TR_ERR_NOPROBLEM = -6,   /* tr_set_problem has not been called */
+  TR_ERR_UNSUPPORTED = -7  /* geometry outside what the kernels stage */
+} tr_status;
+
+typedef enum { TR_LAYOUT_Y = 0, TR_LAYOUT_Z = 1 } tr_layout;
+
+typedef enum {
+  TR_METHOD_BPT = 0,   /* back-projection                    (--method BPT) */
+  TR_METHOD_WBP = 1,   /* R-weighting filter + BPT           (--method WBP) */
+  TR_METHOD_SIRT = 2,  /* SIRT,n,gamma                       */
+  TR_METHOD_SART = 3   /* SART,n,gamma                       */
+} tr_method;
+
+/* Library version: major*10000 + minor*100 + patch. */
+int tr_version(void);
+const char *tr_status_string(int status);
+
+/* Per-tilt coefficients from tilt angles and the --geometry
+ * offset,pitch(XTILT),zshift values, bit-identical to the reference CPU path:
+ * TranslateAngleToCoefficients + DecorateCoefficients
+ * (src/TiltRec/src/main/main-mpi.cpp:85-106, 110-183).  Host only.
+ * coeff8_out: ntilt*8 doubles. */
+tr_status tr_geometry_from_angles(const float *angles_deg, int ntilt,
+                                  float offset, float pitch, float zshift,
+                                  double *coeff8_out);
+
+/* Context on CUDA device `device` with a scratch budget in bytes (0 = none).
+ * Replaces InitializeCuda (src/TiltRec/src/main/main-cuda.cpp:83-109) minus
+ * its cudaDeviceReset. */
+tr_status tr_create(int device, size_t hbm_budget, tr_ctx **out);
+tr_status tr_destroy(tr_ctx *ctx);
+const char *tr_last_error(const tr_ctx *ctx);
+size_t tr_scratch_bytes(const tr_ctx *ctx);
+
+/* Problem geometry: projection stack nx*ny*ntilt, volume thickness, layout,
+ * coefficients (ntilt*8 doubles) and the float origin the reference uses
+ * (TiltRec-mpi: (nx/2, th/2, th/2), main-mpi.cpp:743-745;
+ *  TiltRecZ:     (nx/2, ny/2, th/2), main-mpiz.cpp:1078-1080). */
+tr_status tr_set_problem(tr_ctx *ctx, int nx, int ny, int ntilt,
+                         int thickness, int layout, const double *coeff8,
+                         float ox, float oy, float oz);
+
+/* Replace the coefficients of the current problem (same sizes, e.g. the next
+ * tilt series of the same shape).  Ordered after work already queued on
+ * `stream` (NULL: the context's own stream); invalidates the cached SIRT/SART
+ * weights.  Same validation as tr_set_problem. */
+tr_status tr_update_geometry(tr_ctx *ctx, const double *coeff8, void *stream);
+
+/* R-weighting filter in place over every row of the stack [ntilt][ny][nx]:
+ * ApplyFilterInplace(..., mode 2) (src/TiltRec/src/filter/filter_prj.h:24,
+ * filter_prj.cpp:674-736, 787-795). */
+tr_status tr_filter_rweight(tr_ctx *ctx, float *proj_dev, void *stream);
+
+/* vol += sum over tilts of s/c (normalised bilinear gather) on sections
+ * [z0, z0+nz) of the volume; vol_dev points at section z0 of the layout's
+ * volume.  BackProject (main-mpi.cpp:411-450; main-mpiz.cpp:322-363, which
+ * zeroes the volume first) and CuBackProject / CuBackProjectZ
+ * (recon_y.cuh:25, recon_z.cuh:17). */
+tr_status tr_backproject(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
+                         int z0, int nz, void *stream);
+
+/* Forward projection of sections [z0, z0+nz): val += splat(vol) and, if
+ * wt_dev != NULL, wt += splat(1), for every tilt ([ntilt][ny][nx]).
+ * Reproject (main-mpi.cpp:286-344; main-mpiz.cpp:197-254). */
+tr_status tr_forward_project(tr_ctx *ctx, const float *vol_dev, int z0, int nz,
+                             float *val_dev, float *wt_dev, void *stream);
+
+/* SIRT, `iters` iterations with relaxation gamma, in place on vol_dev (the
+ * starting volume, --initial semantics).  SIRT (main-mpi.cpp:614-664;
+ * main-mpiz.cpp:548-601), CuSIRT / CuSIRTZ (recon_y.cuh:31, recon_z.cuh:22). */
+tr_status tr_sirt(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
+                  int iters, float gamma, void *stream);
+
+/* SART, in place.  SART (main-mpi.cpp:578-612; main-mpiz.cpp:502-546),
+ * CuSART / CuSARTZ (recon_y.cuh:35, recon_z.cuh:26). */
+tr_status tr_sart(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
+                  int iters, float gamma, void *stream);
+
+/* WBP: filter proj_dev in place, then vol += back-projection.
+ * main-mpi.cpp:841-846 (ApplyFilterInplace mode 2 + BackProject), CuFBP with
+ * filterMode 2 (recon_y.cuh:28). */
+tr_status tr_wbp(tr_ctx *ctx, float *proj_dev, float *vol_dev, void *stream);
+
+/* Host-buffer reconstruction, the path a drop-in CLI takes: copies the
+ * projections from host memory, reconstructs with `method` starting from
+ * vol_host (BPT/WBP add to it; pass zeros for a fresh volume) and copies the
+ * volume back; returns when vol_host holds the result.  Pinned host buffers
+ * give the fastest copies.  Device buffers are kept in the context and reused
+ * across calls of the same size. */
+tr_status tr_reconstruct_host(tr_ctx *ctx, int method, const float *proj_host,
+                              float *vol_host, int iters, float gamma);
+
+/* Wait for all work the context issued. */
+tr_status tr_synchronize(tr_ctx *ctx);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TILTREC_B200_H */

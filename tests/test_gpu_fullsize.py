@@ -1,0 +1,137 @@
+"""Full-size checks on the benchmark configurations (GPU).
+
+cfg0 (256^2, 41 tilts, 256x256x64) is small enough for whole-volume parity
+with the oracle.  cfg1 (1024^2, 61 tilts, 1024x1024x256) is checked by
+sampled-row parity -- the oracle reconstructs a crop of rows with margins
+wide enough that the compared rows see the same data -- and by
+size-independent properties: determinism, linearity, adjointness of the
+forward splat and the unnormalised gather, and SIRT convergence."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from autom2_b200 import synth
+from autom2_b200 import tiltrec as T
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def cfg0_data(restatement):
+    cfg = synth.config("cfg0")
+    c8 = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    org = T.default_origin(0, nx, ny, th)
+    g = restatement.geom(nx, ny, nt, th, 0, 0, org)
+    ph = synth.phantom(cfg).numpy()
+    proj = np.zeros((nt, ny, nx), np.float32)
+    for t in range(nt):
+        v, w = restatement.reproject(g, c8[t], ph)
+        proj[t] = np.where(w != 0, v / np.where(w != 0, w, 1), 0)
+    return cfg, c8, org, g, synth.add_noise(proj, cfg)
+
+
+def test_cfg0_wbp_full_volume(engine, restatement, cfg0_data):
+    cfg, c8, org, g, proj = cfg0_data
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    engine.set_problem(nx, ny, nt, th, c8, 0, org)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    engine.wbp(dev(proj), vol)
+    ref = restatement.backproject(g, c8, restatement.filter_rweight(proj),
+                                  np.zeros((ny, th, nx), np.float32))
+    assert O.rel_l2(host(vol), ref) < TOL
+
+
+def _cfg1_problem(engine):
+    cfg = synth.config("cfg1")
+    c8 = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    org = T.default_origin(0, nx, ny, th)
+    engine.set_problem(nx, ny, nt, th, c8, 0, org)
+    return cfg, c8, org
+
+
+def test_cfg1_sampled_rows_sirt(engine, restatement):
+    cfg, c8, org = _cfg1_problem(engine)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    rng = np.random.default_rng(11)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    engine.sirt(dev(proj), vol, 2, 0.5)
+    out = host(vol)
+    for yc in (5, 511, 1017):
+        # Crop rows [ya, yb) of both the volume and the projections: the
+        # compared rows are at least m rows from any crop edge that is not
+        # also an edge of the full problem, more than two iterations of
+        # coupling through the forward splat can reach.
+        R, m = 4, 48
+        ya, yb = max(0, yc - m), min(ny, yc + R + m)
+        o = (org[0], org[1] - ya, org[2])
+        g = restatement.geom(nx, yb - ya, nt, th, 0, 0, o)
+        crop = restatement.sirt(g, c8, proj[:, ya:yb],
+                                np.zeros((yb - ya, th, nx), np.float32), 2, 0.5)
+        got = out[yc:yc + R]
+        want = crop[yc - ya:yc - ya + R]
+        assert O.rel_l2(got, want) < TOL, yc
+
+
+def test_cfg1_back_projection_deterministic_and_linear(engine):
+    cfg, c8, org = _cfg1_problem(engine)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    g = torch.Generator(device="cuda").manual_seed(3)
+    p1 = torch.randn((nt, ny, nx), device="cuda", generator=g)
+    p2 = torch.randn((nt, ny, nx), device="cuda", generator=g)
+    a = torch.zeros((ny, th, nx), device="cuda")
+    b = torch.zeros_like(a)
+    engine.backproject(p1, a)
+    engine.backproject(p1, b)
+    assert torch.equal(a, b)
+    c = torch.zeros_like(a)
+    engine.backproject(2 * p1 + p2, c)
+    d = torch.zeros_like(a)
+    engine.backproject(p2, d)
+    assert O.rel_l2(host(c), host(2 * a + d)) < 1e-6
+
+
+def test_cfg1_forward_projection_linear(engine):
+    cfg, c8, org = _cfg1_problem(engine)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    g = torch.Generator(device="cuda").manual_seed(4)
+    v1 = torch.randn((ny, th, nx), device="cuda", generator=g)
+    v2 = torch.randn((ny, th, nx), device="cuda", generator=g)
+    f = lambda v: (engine.forward_project(v, out := torch.zeros((nt, ny, nx), device="cuda")),  # noqa: E731
+                   out)[1]
+    lhs = f(3 * v1 - v2)
+    rhs = 3 * f(v1) - f(v2)
+    assert O.rel_l2(host(lhs), host(rhs)) < 1e-6
+
+
+def test_cfg1_sirt_converges(engine):
+    """On data from the forward model, SIRT's projection residual falls."""
+    cfg, c8, org = _cfg1_problem(engine)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    ph = synth.phantom(cfg, device="cuda")
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    wt = torch.zeros_like(val)
+    engine.forward_project(ph, val, wt)
+    proj = torch.where(wt != 0, val / torch.where(wt != 0, wt, 1), 0)
+    vol = torch.zeros_like(ph)
+    res = []
+    for _ in range(3):
+        engine.sirt(proj, vol, 2, 0.5)
+        val.zero_()
+        engine.forward_project(vol, val)
+        res.append(float(torch.linalg.vector_norm(
+            torch.where(wt != 0, proj - val / torch.where(wt != 0, wt, 1), 0))))
+    assert res[0] > res[1] > res[2]

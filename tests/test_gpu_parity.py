@@ -1,0 +1,225 @@
+"""Parity of the sm_100a kernels, called through the C ABI, with the
+reference CPU path (golden fixtures) and the oracle restatement (seeded
+random cases).
+
+Tolerance: relative L2 <= 1e-5 against the reference's own float32 CPU path,
+the bar the plain FP32 GPU form must meet.  The kernels interpolate with
+Q32.32 fixed-point coordinates and sum tilts in registers, so they are not
+bit-identical to the reference's per-tilt float updates."""
+import zlib
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from autom2_b200 import tiltrec as T
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+def _dims(g, name):
+    nx, ny, nt, th = (int(v) for v in g[f"{name}/dims"])
+    return nx, ny, nt, th, tuple(float(v) for v in g[f"{name}/origin"])
+
+
+@pytest.mark.parametrize("name", ["ysep", "ygen"])
+def test_golden_y_layout(engine, golden, name):
+    nx, ny, nt, th, org = _dims(golden, name)
+    g = lambda k: golden[f"{name}/{k}"]  # noqa: E731
+    engine.set_problem(nx, ny, nt, th, g("coeff8"), T.LAYOUT_Y, org)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    engine.backproject(dev(g("proj")), vol)
+    assert O.rel_l2(host(vol), g("bpt")) < TOL
+    p = dev(g("proj"))
+    engine.filter_rweight(p)
+    assert O.rel_l2(host(p), g("filtered")) < 2e-6
+    vol.zero_()
+    engine.backproject(p, vol)
+    assert O.rel_l2(host(vol), g("wbp")) < TOL
+    vol = dev(g("vol0"))
+    engine.sirt(dev(g("proj")), vol, 3, 0.5)
+    assert O.rel_l2(host(vol), g("sirt3")) < TOL
+    vol = dev(g("vol0"))
+    engine.sart(dev(g("proj")), vol, 1, 0.5)
+    assert O.rel_l2(host(vol), g("sart1")) < TOL
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    wt = torch.zeros_like(val)
+    engine.forward_project(dev(g("vol0")), val, wt)
+    assert O.rel_l2(host(val)[nt // 2], g("fp_val")) < TOL
+    assert O.rel_l2(host(wt)[nt // 2], g("fp_wt")) < TOL
+
+
+def test_golden_z_layout(engine, golden):
+    nx, ny, nt, th, org = _dims(golden, "zsep")
+    g = lambda k: golden[f"zsep/{k}"]  # noqa: E731
+    engine.set_problem(nx, ny, nt, th, g("coeff8"), T.LAYOUT_Z, org)
+    vol = torch.zeros((th, ny, nx), device="cuda")
+    engine.backproject(dev(g("proj")), vol)
+    assert O.rel_l2(host(vol), g("bpt")) < TOL
+    vol.zero_()
+    engine.wbp(dev(g("proj")), vol)
+    assert O.rel_l2(host(vol), g("wbp")) < TOL
+    vol = dev(g("vol0"))
+    engine.sirt(dev(g("proj")), vol, 2, 0.7)
+    assert O.rel_l2(host(vol), g("sirt2")) < TOL
+
+
+def test_golden_cfg0_scaled(engine, golden):
+    nx, ny, nt, th, org = _dims(golden, "cfg0s4")
+    g = lambda k: golden[f"cfg0s4/{k}"]  # noqa: E731
+    engine.set_problem(nx, ny, nt, th, g("coeff8"), T.LAYOUT_Y, org)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    engine.wbp(dev(g("proj")), vol)
+    assert O.rel_l2(host(vol), g("wbp")) < TOL
+    vol.zero_()
+    engine.sirt(dev(g("proj")), vol, 5, 0.5)
+    assert O.rel_l2(host(vol), g("sirt5")) < TOL
+
+
+# ---------------------------------------------------------------- random cases
+
+CASES = {
+    # name: (nx, ny, nt, th, amax, offset, pitch, zshift, shift_sigma, rot_deg)
+    "sep_shift": (67, 45, 11, 19, 60, 0.0, 0.0, 0.0, 1.0, 0.0),
+    "sep_big_shift": (40, 33, 9, 21, 70, 5.0, 0.0, 3.0, 12.0, 0.0),
+    "steep": (50, 26, 8, 40, 85, 0.0, 0.0, 0.0, 0.5, 0.0),
+    "xtilt": (58, 37, 10, 17, 60, 1.0, 6.0, -2.0, 0.7, 0.0),
+    "rotated": (64, 48, 12, 16, 65, 0.0, 0.3, 0.0, 1.0, 3.0),
+    "big_rotation": (48, 48, 7, 12, 50, 0.0, 0.0, 0.0, 0.0, 25.0),
+}
+
+
+def _random_case(restatement, name, layout):
+    nx, ny, nt, th, amax, off, pitch, zs, sh, rot = CASES[name]
+    rng = np.random.default_rng(zlib.crc32(name.encode()) + layout)
+    ang = np.sort(rng.uniform(-amax, amax, nt)).astype(np.float32)
+    c8 = restatement.coeffs(ang, off, pitch, zs)
+    if rot:
+        psi = np.deg2rad(rng.normal(0, rot, nt))
+        a, b = c8[:, :4].copy(), c8[:, 4:].copy()
+        c8[:, :4] = np.cos(psi)[:, None] * a - np.sin(psi)[:, None] * b
+        c8[:, 4:] = np.sin(psi)[:, None] * a + np.cos(psi)[:, None] * b
+    c8[:, 0] += rng.normal(0, sh, nt)
+    c8[:, 4] += rng.normal(0, sh, nt)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    vshape = (ny, th, nx) if layout == 0 else (th, ny, nx)
+    vol0 = rng.normal(size=vshape).astype(np.float32)
+    org = T.default_origin(layout, nx, ny, th)
+    return nx, ny, nt, th, c8, proj, vol0, org
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("name", list(CASES))
+def test_random_vs_oracle(engine, restatement, name, layout):
+    R = restatement
+    nx, ny, nt, th, c8, proj, vol0, org = _random_case(R, name, layout)
+    g = R.geom(nx, ny, nt, th, layout, 0, org)
+    engine.set_problem(nx, ny, nt, th, c8, layout, org)
+    vol = dev(vol0)
+    engine.backproject(dev(proj), vol)
+    assert O.rel_l2(host(vol), R.backproject(g, c8, proj, vol0)) < TOL
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    wt = torch.zeros_like(val)
+    engine.forward_project(dev(vol0), val, wt)
+    for t in range(nt):
+        v, w = R.reproject(g, c8[t], vol0)
+        assert O.rel_l2(host(val)[t], v) < TOL, t
+        assert O.rel_l2(host(wt)[t], w) < TOL, t
+    vol = dev(vol0)
+    engine.sirt(dev(proj), vol, 2, 0.6)
+    assert O.rel_l2(host(vol), R.sirt(g, c8, proj, vol0, 2, 0.6)) < TOL
+    vol = dev(vol0)
+    engine.sart(dev(proj), vol, 1, 0.4)
+    assert O.rel_l2(host(vol), R.sart(g, c8, proj, vol0, 1, 0.4)) < TOL
+
+
+def test_exact_integer_geometry(engine, restatement):
+    """Tilt 0 with no shift puts every voxel exactly on a detector column
+    (dx = 0): the back-projection is the projection row, copied along z.
+    The kernels interpolate with one FMA, fma(1+dx, s, b-s), which returns b
+    to within one rounding of b-s at dx = 0."""
+    nx, ny, nt, th = 33, 9, 1, 5
+    c8 = restatement.coeffs(np.zeros(1, np.float32))
+    rng = np.random.default_rng(5)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    org = T.default_origin(0, nx, ny, th)
+    engine.set_problem(nx, ny, nt, th, c8, 0, org)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    engine.backproject(dev(proj), vol)
+    out = host(vol)
+    want = np.broadcast_to(proj[0][:, None, :], out.shape)
+    assert O.rel_l2(out, want) < 1e-6
+    assert np.abs(out - want).max() <= 4 * np.finfo(np.float32).eps * np.abs(proj).max()
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_zslabs_add_up(engine, restatement, layout):
+    """Back-projecting z-slabs separately equals the whole volume, and the
+    forward projections of slabs sum to the whole."""
+    nx, ny, nt, th, c8, proj, vol0, org = _random_case(restatement, "rotated", layout)
+    engine.set_problem(nx, ny, nt, th, c8, layout, org)
+    full = torch.zeros(vol0.shape, device="cuda")
+    engine.backproject(dev(proj), full)
+    parts = torch.zeros_like(full)
+    for z0, nz in ((0, 5), (5, 7), (12, th - 12)):
+        view = parts[:, z0:, :] if layout == 0 else parts[z0:]
+        engine.backproject(dev(proj), view, z0, nz)
+    assert O.rel_l2(host(parts), host(full)) < 1e-6
+    v = dev(vol0)
+    whole = torch.zeros((nt, ny, nx), device="cuda")
+    engine.forward_project(v, whole)
+    summed = torch.zeros_like(whole)
+    for z0, nz in ((0, 9), (9, th - 9)):
+        view = v[:, z0:, :] if layout == 0 else v[z0:]
+        engine.forward_project(view, summed, None, z0, nz)
+    assert O.rel_l2(host(summed), host(whole)) < 1e-6
+
+
+@pytest.mark.parametrize("nx", [256, 1024, 4096])
+def test_filter_widths(engine, restatement, nx):
+    rng = np.random.default_rng(nx)
+    rows = rng.normal(size=(1, 9, nx)).astype(np.float32)
+    c8 = restatement.coeffs(np.zeros(1, np.float32))
+    engine.set_problem(nx, 9, 1, 4, c8, 0)
+    p = dev(rows)
+    engine.filter_rweight(p)
+    assert O.rel_l2(host(p), restatement.filter_rweight(rows)) < 2e-6
+
+
+def test_host_buffer_path(engine, golden):
+    """tr_reconstruct_host (host in, host out) equals the device path."""
+    nx, ny, nt, th, org = _dims(golden, "cfg0s4")
+    g = lambda k: golden[f"cfg0s4/{k}"]  # noqa: E731
+    engine.set_problem(nx, ny, nt, th, g("coeff8"), T.LAYOUT_Y, org)
+    vol = np.zeros((ny, th, nx), np.float32)
+    engine.reconstruct_host("WBP", g("proj").copy(), vol)
+    assert O.rel_l2(vol, g("wbp")) < TOL
+    vol[:] = 0
+    engine.reconstruct_host("SIRT", g("proj").copy(), vol, 5, 0.5)
+    assert O.rel_l2(vol, g("sirt5")) < TOL
+
+
+def test_errors_are_reported(engine):
+    with pytest.raises(T.TiltRecError):
+        engine.set_problem(0, 4, 1, 4, np.zeros((1, 8)))
+    engine.set_problem(16, 8, 1, 4, np.array([[0, 1, 0, 0, 0, 0, 1, 0.]]))
+    with pytest.raises(T.TiltRecError):
+        engine.backproject(torch.zeros(1, device="cuda"), torch.zeros(1, device="cuda"), 3, 5)
+    small = T.Engine(0, hbm_budget=1024)
+    small.set_problem(64, 64, 4, 8, np.tile([[0, 1, 0, 0, 0, 0, 1, 0.]], (4, 1)))
+    with pytest.raises(T.TiltRecError) as e:
+        small.sirt(torch.zeros((4, 64, 64), device="cuda"),
+                   torch.zeros((64, 8, 64), device="cuda"), 1, 0.5)
+    assert e.value.status == -3  # TR_ERR_BUDGET
+    small.close()

@@ -1,0 +1,141 @@
+"""The oracle restatement pinned against the reference (CPU only).
+
+The reference has no tests or golden vectors for TiltRec; the pins are the
+reference's own CPU routines compiled from its sources (live, where
+oracle/_ref is built) and the fixtures they generated (tests/golden)."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _case(g, name):
+    nx, ny, nt, th = (int(v) for v in g[f"{name}/dims"])
+    return nx, ny, nt, th, tuple(float(v) for v in g[f"{name}/origin"])
+
+
+def test_golden_manifest(golden):
+    with open(os.path.join(HERE, "golden", "MANIFEST.json")) as f:
+        man = json.load(f)
+    assert set(man) == set(golden)
+    for k, v in golden.items():
+        assert hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest() == man[k], k
+
+
+@pytest.mark.parametrize("name", ["ysep", "ygen"])
+def test_restatement_matches_reference_y(golden, restatement, name):
+    R = restatement
+    nx, ny, nt, th, org = _case(golden, name)
+    c8 = golden[f"{name}/coeff8"]
+    proj, vol0 = golden[f"{name}/proj"], golden[f"{name}/vol0"]
+    g = R.geom(nx, ny, nt, th, 0, 0, org)
+    zero = np.zeros_like(vol0)
+    # bit for bit: same float operations in the same order as the reference
+    np.testing.assert_array_equal(R.backproject(g, c8, proj, zero), golden[f"{name}/bpt"])
+    np.testing.assert_array_equal(R.sirt(g, c8, proj, vol0, 3, 0.5), golden[f"{name}/sirt3"])
+    np.testing.assert_array_equal(R.sart(g, c8, proj, vol0, 1, 0.5), golden[f"{name}/sart1"])
+    v, w = R.reproject(g, c8[nt // 2], vol0)
+    np.testing.assert_array_equal(v, golden[f"{name}/fp_val"])
+    np.testing.assert_array_equal(w, golden[f"{name}/fp_wt"])
+    # the filter runs its transform in double here, in float in the reference
+    f = R.filter_rweight(proj)
+    assert O.rel_l2(f, golden[f"{name}/filtered"]) < 2e-7
+    assert O.rel_l2(R.backproject(g, c8, f, zero), golden[f"{name}/wbp"]) < 2e-7
+
+
+def test_restatement_matches_reference_z(golden, restatement):
+    R = restatement
+    nx, ny, nt, th, org = _case(golden, "zsep")
+    c8, proj, vol0 = golden["zsep/coeff8"], golden["zsep/proj"], golden["zsep/vol0"]
+    g = R.geom(nx, ny, nt, th, 1, 0, org)
+    zero = np.zeros_like(vol0)
+    np.testing.assert_array_equal(R.backproject(g, c8, proj, zero), golden["zsep/bpt"])
+    np.testing.assert_array_equal(R.sirt(g, c8, proj, vol0, 2, 0.7), golden["zsep/sirt2"])
+    wbp = R.backproject(g, c8, R.filter_rweight(proj), zero)
+    assert O.rel_l2(wbp, golden["zsep/wbp"]) < 2e-7
+
+
+def test_restatement_cfg0_scaled(golden, restatement):
+    R = restatement
+    nx, ny, nt, th, org = _case(golden, "cfg0s4")
+    c8, proj = golden["cfg0s4/coeff8"], golden["cfg0s4/proj"]
+    g = R.geom(nx, ny, nt, th, 0, 0, org)
+    zero = np.zeros((ny, th, nx), np.float32)
+    np.testing.assert_array_equal(R.sirt(g, c8, proj, zero, 5, 0.5), golden["cfg0s4/sirt5"])
+    wbp = R.backproject(g, c8, R.filter_rweight(proj), zero)
+    assert O.rel_l2(wbp, golden["cfg0s4/wbp"]) < 2e-7
+
+
+def test_geometry_restatement_matches_reference(golden, restatement):
+    ang = golden["geom/angles"]
+    for par, c20 in zip(golden["geom/params"], golden["geom/coeff20"]):
+        c8 = restatement.coeffs(ang, *par)
+        np.testing.assert_array_equal(c8, c20[:, [0, 1, 2, 3, 10, 11, 12, 13]])
+        assert not np.any(c20[:, 4:10]) and not np.any(c20[:, 14:20])
+
+
+def test_fp64_oracle_agrees_with_fp32(golden, restatement):
+    R = restatement
+    nx, ny, nt, th, org = _case(golden, "cfg0s4")
+    c8, proj = golden["cfg0s4/coeff8"], golden["cfg0s4/proj"]
+    g = R.geom(nx, ny, nt, th, 0, 0, org)
+    zero = np.zeros((ny, th, nx), np.float32)
+    a = R.sirt(g, c8, proj, zero, 3, 0.5)
+    b = R.sirt(g, c8, proj.astype(np.float64), zero.astype(np.float64), 3, 0.5, fp64=True)
+    assert O.rel_l2(a, b) < 1e-5
+
+
+def _filter_numpy(rows):
+    """Independent float64 restatement of filter_Rweighting_1D_many
+    (filter/filter_prj.cpp:674-736) with numpy's FFT."""
+    nx = rows.shape[-1]
+    N = nx + nx // 10
+    nxp = N - nx + 1
+    r = int(np.floor(np.float32(N) * np.float32(0.05)))
+    sg = np.float32(N) * np.float32(0.5)
+    x = rows.reshape(-1, nx).astype(np.float64)
+    j = np.arange(nx, N)
+    wa = (j - nx + 1).astype(np.float32) / np.float32(nxp)
+    wb = (N - j).astype(np.float32) / np.float32(nxp)
+    pad = np.concatenate([x, wa * x[:, :1] + wb * x[:, -1:]], axis=1)
+    X = np.fft.rfft(pad, axis=1)
+    k = np.arange(X.shape[1])
+    W = np.where(k <= r, k, r * np.exp(-((k - r) ** 2).astype(np.float32) / (sg * sg)))
+    W = W.astype(np.float64)
+    W[0] = 0.2
+    y = np.fft.irfft(X * W, n=N, axis=1) * N / nx
+    return y[:, :nx].reshape(rows.shape)
+
+
+@pytest.mark.parametrize("nx", [37, 64, 256, 333])
+def test_filter_restatement_vs_numpy(restatement, nx):
+    rng = np.random.default_rng(nx)
+    rows = rng.normal(size=(5, 7, nx)).astype(np.float32)
+    a = restatement.filter_rweight(rows)
+    b = _filter_numpy(rows)
+    assert O.rel_l2(a, b) < 1e-6
+
+
+def test_reference_live_random_case(reference, restatement):
+    """Fresh seeded inputs through both (where oracle/_ref is built)."""
+    rng = np.random.default_rng(99)
+    nx, ny, nt, th = 29, 17, 6, 9
+    ang = rng.uniform(-80, 80, nt).astype(np.float32)
+    c8 = restatement.coeffs(ang, -1.5, 7.0, 2.0)
+    c8[:, 0] += rng.normal(0, 3, nt)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    vol = rng.normal(size=(ny, th, nx)).astype(np.float32)
+    org = (nx * 0.5, th * 0.5, th * 0.5)
+    g = restatement.geom(nx, ny, nt, th, 0, 0, org)
+    np.testing.assert_array_equal(
+        restatement.backproject(g, c8, proj, vol),
+        reference.y_backproject(nx, ny, nt, th, O.coeff20(c8), org, proj, vol))
+    np.testing.assert_array_equal(
+        restatement.sirt(g, c8, proj, vol, 2, 0.3),
+        reference.y_sirt(nx, ny, nt, th, O.coeff20(c8), org, proj, vol, 2, 0.3))
