@@ -1,0 +1,391 @@
+"""Benchmark: plain FP32 SIRT-30 (relaxation 0.5) on the 1024^2 x 61-tilt
+tilt series, volume 1024 x 1024 x 256 (the SIRT configuration), through the
+TiltRec B200 engine's C ABI.
+
+One step = one complete reconstruction: upload of the series' geometry
+(which also recomputes its projection and voxel weights), a zeroed volume and
+30 SIRT iterations (forward splat, residual, back-projection and update).
+Metric: voxel-projection updates per second (VPU/s; each SIRT iteration
+counts 2 x tilts x voxels).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one independent reconstruction per GPU (one process per GPU under
+torchrun; the path needs no exchange between series), scaling "weak".
+
+--impl reference times the reference's own CPU implementation of the path
+(the compiled reference sources in oracle/_ref, else the oracle restatement)
+on the host's cores, on a bounded row sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "voxel-proj updates/s"
+UNIT = "VPU/s"
+WORKLOAD = "SIRT-30 FP32, 61 tilts 1024x1024, volume 1024x1024x256 (cfg1)"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary
+    (profiles/<kernel>.md, line 'traffic_bytes_per_launch: N'), or None."""
+    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed
+    region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax = float(p[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_series(eng, torch, cfg, coeff):
+    """Synthetic cfg1 tilt series on the device: ellipsoid + bead phantom,
+    projected with the engine's forward model (val/wt), plus Gaussian noise
+    of 0.3 x std.  Input generation only; it is outside the timed region."""
+    from autom2_b200 import synth
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    ph = synth.phantom(cfg, device="cuda")
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    wt = torch.zeros_like(val)
+    eng.forward_project(ph, val, wt)
+    proj = torch.where(wt != 0, val / torch.where(wt != 0, wt, 1), 0)
+    g = torch.Generator(device="cuda").manual_seed(cfg.seed + 7)
+    proj += cfg.noise * proj.std() * torch.randn(proj.shape, device="cuda", generator=g)
+    del ph, val, wt
+    torch.cuda.synchronize()
+    return proj.contiguous()
+
+
+def cpu_baseline(cfg, coeff, proj_np, target_s: float = 12.0):
+    """The reference SIRT on a bounded row sample, all host threads.  Each
+    thread owns an even share of the sampled rows plus the reference's XTILT
+    halo (ceil(|tan(pitch)| * th) rows per side, as a TiltRec-mpi rank does);
+    every row a thread reconstructs counts as work."""
+    import math
+
+    import oracle
+    nthreads = os.cpu_count() or 1
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    halo = math.ceil(abs(math.tan(math.radians(cfg.xtilt))) * th)
+
+    def rows_done(r0, rows):
+        base, rem = divmod(rows, nthreads)
+        total = 0
+        for r in range(nthreads):
+            s = r0 + r * base + min(r, rem)
+            e = s + base + (1 if r < rem else 0)
+            if e > s:
+                total += (e - s) + min(halo, s) + min(halo, ny - e)
+        return total
+
+    if oracle.reference_available():
+        ref = oracle.Reference()
+        c20 = oracle.coeff20(coeff)
+        kind = "reference"
+
+        def run(rows):
+            r0 = ny // 2 - rows // 2
+            t = ref.y_sirt_threaded(nthreads, nx, ny, nt, th, c20, cfg.xtilt, proj_np,
+                                    r0, rows, 1, cfg.gamma)
+            return t, rows_done(r0, rows)
+    else:
+        R = oracle.Restatement()
+        kind = "port"
+
+        def run(rows):
+            r0 = ny // 2 - rows // 2
+            o = (nx * 0.5, th * 0.5 - r0, th * 0.5)
+            g = R.geom(nx, rows, nt, th, 0, 0, o)
+            t0 = time.perf_counter()
+            R.sirt(g, coeff, proj_np[:, r0:r0 + rows].copy(),
+                   np.zeros((rows, th, nx), np.float32), 1, cfg.gamma)
+            return time.perf_counter() - t0, rows
+    rows = nthreads
+    t, done = run(rows)
+    per_row = t / max(1.0, done / nthreads)          # seconds per row per thread
+    want = max(1, int(target_s / per_row) - 2 * halo)  # rows per thread
+    rows = min(ny - 2 * halo, want * nthreads)
+    if rows > nthreads:
+        t, done = run(rows)
+    vpu = 2.0 * nt * done * th * nx
+    return {"value": vpu / t, "unit": UNIT, "cores": nthreads, "kind": kind,
+            "sample": f"1 SIRT iteration of the cfg1 series on {rows} of {ny} rows "
+                      f"({done} rows incl. XTILT halos, {nthreads} threads), {t:.1f} s"}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from autom2_b200 import synth
+    cfg = synth.config("cfg1")
+    coeff = synth.coefficients(cfg)
+    rng = np.random.default_rng(1)
+    # The CPU arm reconstructs row samples of the same series shape; the
+    # input values do not change its timing.
+    proj = rng.normal(size=(cfg.ntilt, cfg.ny, cfg.nx)).astype(np.float32)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(cfg, coeff, proj, target_s=6.0 if i < args.warmup else 10.0)
+        if i >= args.warmup:
+            vals.append(b)
+    value = statistics.median(v["value"] for v in vals)
+    cb = dict(vals[-1])
+    cb["value"] = value
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+    build.build_lib()
+    cfg = synth.config("cfg1")
+    coeff = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    eng = T.Engine(dev)
+    eng.set_problem(nx, ny, nt, th, coeff, T.LAYOUT_Y)
+    proj = make_series(eng, torch, cfg, coeff)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    vpu_step = 2.0 * cfg.iters * nt * nx * ny * th
+    stream = torch.cuda.current_stream()
+
+    def step():
+        eng.update_geometry(coeff)
+        vol.zero_()
+        eng.sirt(proj, vol, cfg.iters, cfg.gamma)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    # L2 (126 MB) holds a small part of the 1 GB volume and 256 MB stack
+    # that every pass streams, so no extra flush is needed between steps.
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * vpu_step / (ms / 1e3)
+
+    # Roofline of the dominant kernel (back-projection with SIRT update).
+    # Algorithmic bytes per launch: residual stack (nt*ny*nx*4, staged once
+    # per tile window from L2) + voxel weights read (4 B/voxel) + volume
+    # read and write (8 B/voxel).
+    hbm, peak_kind = peaks()
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    nvox = nx * ny * th
+    bp_bytes = nt * ny * nx * 4 + nvox * 12
+    fp_bytes = nvox * 4 + nt * ny * nx * 4
+    reps = 5
+    eng.sirt(proj, vol, 1, cfg.gamma)  # weights ready, resid in scratch
+    torch.cuda.synchronize()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    for _ in range(reps):
+        eng.backproject(proj, vol)
+    b1.record(stream)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(reps):
+        eng.forward_project(vol, val)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    bp_ms = b0.elapsed_time(b1) / reps
+    fp_ms = f0.elapsed_time(f1) / reps
+    # bytes for the timed normalised back-projection: stack + volume RMW
+    bpn_bytes = nt * ny * nx * 4 + nvox * 8
+    dominant = "fp_kernel" if fp_ms > bp_ms else "bp_kernel"
+    kms, kbytes = (fp_ms, fp_bytes) if fp_ms > bp_ms else (bp_ms, bpn_bytes)
+    achieved = kbytes / (kms / 1e3) / 1e9
+    traffic = profile_traffic(dominant)
+    vpu_kernel = nt * nvox
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": traffic, "kernel": dominant,
+                "peak_source": peak_kind,
+                "kernel_ms": kms, "kernel_vpu_per_s": vpu_kernel / (kms / 1e3),
+                "fp_ms": fp_ms, "bp_ms": bp_ms,
+                "note": "back-projection and forward splat are FP32-issue and "
+                        "shared-memory bound (no tensor-core form); HBM fraction "
+                        "reported as asked"}
+
+    # End to end through the C ABI with host buffers: geometry, H2D of the
+    # stack and the starting volume, 30 iterations, D2H of the volume.
+    proj_h = proj.cpu().pin_memory()
+    vol_h = torch.zeros((ny, th, nx)).pin_memory()
+    proj_np, vol_np = proj_h.numpy(), vol_h.numpy()
+    e2e_steps = max(1, min(args.steps, 3))
+    eng.update_geometry(coeff)
+    eng.reconstruct_host("SIRT", proj_np, vol_np, cfg.iters, cfg.gamma)  # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        eng.update_geometry(coeff)
+        vol_np[:] = 0
+        eng.reconstruct_host("SIRT", proj_np, vol_np, cfg.iters, cfg.gamma)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": ws * vpu_step / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(proj_np.nbytes + vol_np.nbytes),
+           "d2h_bytes_per_step": int(vol_np.nbytes), "ms_per_step": e2e_s * 1e3}
+
+    line = None
+    if rank == 0:
+        cb = cpu_baseline(cfg, coeff, proj.cpu().numpy()) if ws == 1 else None
+        launches_per_step = 2 + 3 * cfg.iters  # weights (fp, bp) + (fp, resid, bp)/iter
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "method": "SIRT", "iters": cfg.iters,
+                           "gamma": cfg.gamma, "tilts": nt, "proj": [ny, nx],
+                           "volume": [nx, ny, th], "layout": "Y",
+                           "l2": "inputs larger than L2 (1.07 GB volume, 256 MB stack)",
+                           "parallelism": f"replicas x{ws}"},
+                "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
+                "gpu_launches": launches_per_step * args.steps,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
