@@ -1,0 +1,242 @@
+// tr_sirt_static: SIRT for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc at the point where they reconstruct:
+// a host application whose memory pool already owns the device memory it is
+// allowed to use (a serving process holding a fixed HBM budget, a framework's
+// caching allocator), or code that must not issue the device-wide
+// synchronisation a cudaMalloc/cudaFree can imply in the middle of a
+// stream-ordered pipeline.  This entry point needs no context and allocates
+// nothing: its scratch (the per-tilt geometry, the reprojection, the
+// projection weights and the voxel weights) lives in one file-scope static
+// device array of kStaticScratchBytes (64 MiB).
+//
+// The array is reserved on a device when this file's device module is loaded
+// there -- with CUDA's lazy module loading, at this entry point's first call on
+// that device -- and stays reserved until the process exits.  That first call
+// also looks up the array's device address (cudaGetSymbolAddress, with the
+// device current); make it before any stream capture.  Every call shares the
+// one array and leaves the last call's contents in it: the buffers that must
+// start at zero are cleared by each call, and calls whose work overlaps on the
+// GPU (different streams, or different host threads) race on the scratch and
+// must be serialised by the caller.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "tiltrec_b200.h"
+#include "tr_internal.cuh"
+
+namespace trb {
+cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
+cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
+cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
+                         int nsm, cudaStream_t s);
+}  // namespace trb
+
+using namespace trb;
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = 64ull << 20;
+constexpr int kStaticMaxTilts = 360;
+constexpr int kStaticMaxDevices = 64;
+constexpr size_t kStaticSmemBp = 64 * 1024;
+constexpr size_t kStaticSmemFp = 48 * 1024;
+constexpr size_t kStaticSmemMax = 200 * 1024;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+
+std::mutex g_static_mu;
+void *g_static_addr[kStaticMaxDevices];
+
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Device address of the static scratch on `device` (which is current).
+cudaError_t static_scratch(int device, void **out) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_addr[device] = p;
+  }
+  *out = g_static_addr[device];
+  return cudaSuccess;
+}
+
+struct StaticGeom {
+  int fw, fh, chunk_bp, chunk_fp;
+  bool sep;
+};
+
+// Fixed-point steps and tile windows for the coefficients, as the context
+// path derives them; returns false when the geometry is outside what the
+// kernels stage.
+bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
+            StaticGeom *out) {
+  bool sep = true;
+  double span_u = 0, span_v = 0;
+  const double two32 = 4294967296.0;
+  const double ext = std::max(std::max(nx, ny), th) + 64.0;
+  for (int t = 0; t < nt; ++t) {
+    const double *k = coeff8 + 8 * (size_t)t;
+    for (int i = 0; i < 4; ++i) {
+      if (!std::isfinite(k[i]) || !std::isfinite(k[4 + i])) return false;
+      g[t].a[i] = k[i];
+      g[t].b[i] = k[4 + i];
+    }
+    for (int i = 0; i < 3; ++i) {
+      if (fabs(k[1 + i]) > 1024.0 || fabs(k[5 + i]) > 1024.0) return false;
+      g[t].A[i] = llrint(k[1 + i] * two32);
+      g[t].B[i] = llrint(k[5 + i] * two32);
+    }
+    if (fabs(k[0]) + (fabs(k[1]) + fabs(k[2]) + fabs(k[3])) * 2 * ext > 1.0e9 ||
+        fabs(k[4]) + (fabs(k[5]) + fabs(k[6]) + fabs(k[7])) * 2 * ext > 1.0e9)
+      return false;
+    if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
+    span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
+                                  fabs(k[3]) * (kTZ - 1));
+    span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
+                                  fabs(k[7]) * (kTZ - 1));
+  }
+  out->fw = (int)ceil(span_u) + 4;
+  out->fh = sep ? kTY : (int)ceil(span_v) + 5;
+  out->sep = sep;
+  const size_t ent_bp = (size_t)out->fw * out->fh * sizeof(float2);
+  const size_t ent_fp = (size_t)out->fw * out->fh * sizeof(float);
+  if (ent_bp > kStaticSmemMax) return false;
+  out->chunk_bp =
+      (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemBp / ent_bp));
+  out->chunk_fp =
+      (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemFp / ent_fp));
+  return true;
+}
+
+tr_status run(int device, int nx, int ny, int nt, int th, int layout,
+              const double *coeff8, float ox, float oy, float oz,
+              const float *proj, float *vol, int iters, float gamma,
+              cudaStream_t s) {
+  const size_t plane = (size_t)nx * ny * nt, nvox = (size_t)nx * ny * th;
+  const size_t geo_b = round256(sizeof(TiltGeo) * nt);
+  const size_t plane_b = round256(plane * sizeof(float));
+  const size_t vox_b = round256(nvox * sizeof(float));
+  if (geo_b + 2 * plane_b + vox_b > kStaticScratchBytes) return TR_ERR_BUDGET;
+
+  TiltGeo g[kStaticMaxTilts];
+  StaticGeom sg;
+  if (!derive(coeff8, nt, nx, ny, th, g, &sg)) return TR_ERR_UNSUPPORTED;
+
+  void *base = nullptr;
+  if (static_scratch(device, &base) != cudaSuccess) return TR_ERR_CUDA;
+  unsigned char *b = (unsigned char *)base;
+  TiltGeo *geo = (TiltGeo *)b;
+  float *wt = (float *)(b + geo_b);
+  float *val = (float *)(b + geo_b + plane_b);
+  float *wtvol = (float *)(b + geo_b + 2 * plane_b);
+
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  // The pageable copy returns once `g` is staged, so the stack buffer may go.
+  if (cudaMemcpyAsync(geo, g, sizeof(TiltGeo) * nt, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return TR_ERR_CUDA;
+
+  VolView v;
+  v.vol = vol;
+  v.nx = nx;
+  v.ny = ny;
+  v.nz = th;
+  v.zoff = 0;
+  v.sy = layout == TR_LAYOUT_Y ? (long long)th * nx : nx;
+  v.sz = layout == TR_LAYOUT_Y ? nx : (long long)ny * nx;
+
+  FpArgs f;
+  f.v = v;
+  f.tstride = (long long)nx * ny;
+  f.pnx = nx;
+  f.pny = ny;
+  f.geo = geo;
+  f.t0 = 0;
+  f.nt = nt;
+  f.ox = ox;
+  f.oy = oy;
+  f.oz = oz;
+  f.fw = sg.fw;
+  f.fh = sg.fh;
+  f.chunk = sg.chunk_fp;
+
+  BpArgs bp;
+  bp.v = v;
+  bp.img.nx = nx;
+  bp.img.ny = ny;
+  bp.img.tstride = (long long)nx * ny;
+  bp.geo = geo;
+  bp.t0 = 0;
+  bp.nt = nt;
+  bp.ox = ox;
+  bp.oy = oy;
+  bp.oz = oz;
+  bp.fw = sg.fw;
+  bp.fh = sg.fh;
+  bp.chunk = sg.chunk_bp;
+  bp.wtvol = wtvol;
+
+  // Geometry-only weights: splat of ones (projection side) and Σ_t c_t
+  // (voxel side); the previous call's contents are cleared first.
+  if (cudaMemsetAsync(wt, 0, plane * sizeof(float), s) != cudaSuccess) return TR_ERR_CUDA;
+  FpArgs fw_ = f;
+  fw_.v.vol = nullptr;
+  fw_.val = wt;
+  if (launch_fp(sg.sep, fw_, s) != cudaSuccess) return TR_ERR_CUDA;
+  BpArgs bw = bp;
+  bw.v.vol = wtvol;
+  bw.img.p = nullptr;
+  bw.gamma = 1.f;
+  bw.out = wtvol;
+  if (launch_bp(BP_WEIGHTS, sg.sep, bw, s) != cudaSuccess) return TR_ERR_CUDA;
+
+  for (int it = 0; it < iters; ++it) {
+    if (cudaMemsetAsync(val, 0, plane * sizeof(float), s) != cudaSuccess)
+      return TR_ERR_CUDA;
+    FpArgs fi = f;
+    fi.val = val;
+    if (launch_fp(sg.sep, fi, s) != cudaSuccess) return TR_ERR_CUDA;
+    if (launch_resid(proj, val, wt, plane, nsm, s) != cudaSuccess) return TR_ERR_CUDA;
+    BpArgs bi = bp;
+    bi.img.p = val;
+    bi.gamma = gamma;
+    bi.out = nullptr;
+    if (launch_bp(BP_SIRT, sg.sep, bi, s) != cudaSuccess) return TR_ERR_CUDA;
+  }
+  return TR_OK;
+}
+
+}  // namespace
+
+extern "C" tr_status tr_sirt_static(int device, int nx, int ny, int ntilt,
+                                    int thickness, int layout,
+                                    const double *coeff8, float ox, float oy,
+                                    float oz, const float *proj_dev,
+                                    float *vol_dev, int iters, float gamma,
+                                    void *stream) {
+  if (nx < 2 || ny < 1 || ntilt < 1 || thickness < 1 || iters < 0 || !coeff8 ||
+      !proj_dev || !vol_dev || ntilt > kStaticMaxTilts || device < 0 ||
+      device >= kStaticMaxDevices || ny > 65535 * kTY ||
+      (layout != TR_LAYOUT_Y && layout != TR_LAYOUT_Z))
+    return TR_ERR_ARG;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return TR_ERR_CUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return TR_ERR_CUDA;
+  const tr_status st = run(device, nx, ny, ntilt, thickness, layout, coeff8, ox, oy,
+                           oz, proj_dev, vol_dev, iters, gamma, (cudaStream_t)stream);
+  if (prev != device) cudaSetDevice(prev);
+  return st;
+}
+
+extern "C" size_t tr_static_scratch_limit(void) { return kStaticScratchBytes; }

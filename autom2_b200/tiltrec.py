@@ -225,3 +225,29 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")
+
+
+def sirt_static(proj, vol, coeff8, iters, gamma, layout=LAYOUT_Y, origin=None,
+                device=0):
+    """SIRT through tr_sirt_static, the entry point that allocates no device
+    memory (its scratch is a 64 MiB static device array; see the header).
+    proj, vol: CUDA tensors; vol is updated in place."""
+    lib = load_library()
+    fn = lib.tr_sirt_static
+    vp, i, f = C.c_void_p, C.c_int, C.c_float
+    fn.argtypes = [i, i, i, i, i, i, C.POINTER(C.c_double), f, f, f, vp, vp, i, f, vp]
+    fn.restype = i
+    nt, ny, nx = proj.shape
+    th = vol.shape[1] if layout == LAYOUT_Y else vol.shape[0]
+    c = np.ascontiguousarray(coeff8, np.float64).reshape(nt, 8)
+    ox, oy, oz = origin if origin is not None else default_origin(layout, nx, ny, th)
+    st = fn(device, nx, ny, nt, th, layout, c.ctypes.data_as(C.POINTER(C.c_double)),
+            ox, oy, oz, proj.data_ptr(), vol.data_ptr(), iters, gamma, _stream(device))
+    if st:
+        raise TiltRecError(st, "tr_sirt_static: " + lib.tr_status_string(st).decode())
+
+
+def static_scratch_limit() -> int:
+    lib = load_library()
+    lib.tr_static_scratch_limit.restype = C.c_size_t
+    return int(lib.tr_static_scratch_limit())

@@ -142,6 +142,27 @@ tr_status tr_wbp(tr_ctx *ctx, float *proj_dev, float *vol_dev, void *stream);
 tr_status tr_reconstruct_host(tr_ctx *ctx, int method, const float *proj_host,
                               float *vol_host, int iters, float gamma);
 
+/* SIRT that allocates no device memory and needs no context.  No
+ * counterpart in the reference.  For callers that cannot call cudaMalloc
+ * where they reconstruct: a process whose memory pool already owns the device
+ * memory it may use, or a stream-ordered pipeline that must not take the
+ * device-wide synchronisation an allocation can imply.  Arguments are those of
+ * tr_set_problem followed by those of tr_sirt; `device` is made current for
+ * the call and restored.  All scratch lives in one static device array of
+ * tr_static_scratch_limit() bytes (64 MiB), reserved on each device the first
+ * time this is called there and held until the process exits; problems whose
+ * geometry (ntilt*112 B), reprojection and projection weights
+ * (2*ntilt*ny*nx*4 B) and voxel weights (voxels*4 B), each rounded up to
+ * 256 B, exceed it are rejected with TR_ERR_BUDGET, and ntilt is at most 360.
+ * The first call on a device looks up the array's device address; make it
+ * before any stream capture.  Calls share the array: each clears what must
+ * start at zero, and calls whose work overlaps on the GPU race. */
+tr_status tr_sirt_static(int device, int nx, int ny, int ntilt, int thickness,
+                         int layout, const double *coeff8, float ox, float oy,
+                         float oz, const float *proj_dev, float *vol_dev,
+                         int iters, float gamma, void *stream);
+size_t tr_static_scratch_limit(void);
+
 /* Wait for all work the context issued. */
 tr_status tr_synchronize(tr_ctx *ctx);
 
