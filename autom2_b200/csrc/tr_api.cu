@@ -51,6 +51,8 @@ struct tr_ctx {
   float ox = 0, oy = 0, oz = 0;
   bool sep = false;
   int fw = 0, fh = 0, chunk_bp = 1, chunk_fp = 1;
+  int ffw = 0, ffh = 0;  // forward-projection tile window
+  float fp_nbound = 0;   // most voxel contributions per forward window entry
   TiltGeo *geo_d = nullptr;
 
   // scratch
@@ -182,9 +184,10 @@ FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
   a.ox = c->ox;
   a.oy = c->oy;
   a.oz = c->oz;
-  a.fw = c->fw;
-  a.fh = c->fh;
+  a.fw = c->ffw;
+  a.fh = c->ffh;
   a.chunk = c->chunk_fp;
+  a.nbound = c->fp_nbound;
   return a;
 }
 
@@ -267,6 +270,16 @@ tr_status build_filter(tr_ctx *c, int nx) {
   return TR_OK;
 }
 
+// Most voxels of one forward-projection tile that can add to one window entry:
+// along x a row of voxels steps the detector column by |a1|, so at most
+// floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their lower
+// column at q-1 or q; every (y, z) row of the tile may contribute.
+float fp_entry_bound(double min_a1) {
+  double nx = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
+  nx = std::min(nx, (double)kFX);
+  return (float)(nx * kTY * kFTZ);
+}
+
 // Validates coefficients, derives the fixed-point steps and the per-tile
 // detector window, and uploads them (ordered on `s`).  Invalidates the cached
 // SIRT/SART weights, which depend on the geometry.
@@ -274,7 +287,7 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   const int nt = c->nt;
   std::vector<TiltGeo> g(nt);
   bool sep = true;
-  double span_u = 0, span_v = 0;
+  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
   const double two32 = 4294967296.0;
   const double ext = std::max(std::max(c->nx, c->ny), c->th) + 64.0;
   for (int t = 0; t < nt; ++t) {
@@ -298,18 +311,25 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
     if (reach_u > 1.0e9 || reach_v > 1.0e9)
       return fail(c, TR_ERR_UNSUPPORTED, "detector coordinates out of range at tilt %d", t);
     if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
+    min_a1 = std::min(min_a1, fabs(k[1]));
     span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
                                   fabs(k[3]) * (kTZ - 1));
     span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
                                   fabs(k[7]) * (kTZ - 1));
+    fspan_u = std::max(fspan_u, fabs(k[1]) * (kFX - 1) + fabs(k[2]) * (kTY - 1) +
+                                    fabs(k[3]) * (kFTZ - 1));
+    fspan_v = std::max(fspan_v, fabs(k[5]) * (kFX - 1) + fabs(k[6]) * (kTY - 1) +
+                                    fabs(k[7]) * (kFTZ - 1));
   }
   const int fw = (int)ceil(span_u) + 4;
   const int fh = sep ? kTY : (int)ceil(span_v) + 5;
+  const int ffw = (int)ceil(fspan_u) + 4;
+  const int ffh = sep ? kTY : (int)ceil(fspan_v) + 5;
   const size_t ent_bp = (size_t)fw * fh * sizeof(float2);
-  const size_t ent_fp = (size_t)fw * fh * sizeof(float);
-  if (ent_bp > kSmemMax)
+  const size_t ent_fp = (size_t)ffw * ffh * sizeof(float);
+  if (ent_bp > kSmemMax || ent_fp > kSmemMax)
     return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds shared memory",
-                fw, fh);
+                ffw, ffh);
   if (s) {
     TR_CUDA(c, cudaMemcpyAsync(c->geo_d, g.data(), sizeof(TiltGeo) * nt,
                                cudaMemcpyHostToDevice, s));
@@ -319,6 +339,9 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   }
   c->fw = fw;
   c->fh = fh;
+  c->ffw = ffw;
+  c->ffh = ffh;
+  c->fp_nbound = fp_entry_bound(min_a1);
   c->sep = sep;
   c->chunk_bp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemBp / ent_bp));
   c->chunk_fp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemFp / ent_fp));

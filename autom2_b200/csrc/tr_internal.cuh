@@ -17,6 +17,12 @@ constexpr int kNV = 16;                       // voxels per thread along z
 constexpr int kTZ = kZG * kNV;                // 32
 constexpr int kMaxChunk = 32;                 // tilts staged per chunk (max)
 
+// Forward-projection tile: each lane owns a pair of neighbouring x voxels, so
+// a warp covers 64 x; rows and z groups as above.
+constexpr int kFX = 2 * kTX;                  // 64
+constexpr int kFNV = 16;                      // voxel pairs per thread along z
+constexpr int kFTZ = kZG * kFNV;              // 32
+
 // Per-tilt projection geometry.  a/b are the reference's linear coefficients
 // (detector x = a0 + a1 X + a2 Y + a3 Z + ox, y likewise with b, X/Y/Z the
 // voxel offsets from the origin).  A/B are the same slopes in Q32.32 fixed
@@ -71,6 +77,7 @@ struct FpArgs {
   int t0, nt;
   float ox, oy, oz;
   int fw, fh, chunk;
+  float nbound;       // most voxel contributions one window entry can collect
 };
 
 // Footprint bookkeeping of one tilt for one tile, computed in FP64.
@@ -79,7 +86,7 @@ struct TileTilt {
                      // relative to (kmin, jmin)
   int kmin, jmin;    // detector column / row of table entry (0, 0)
   int check_rows;    // rows outside [-1, ny-1] are reachable (BP_NORM only)
-  int pad;
+  int nq, nr;        // columns / rows of the window this tile can reach
 };
 
 // Separable rows (b1 = b3 = 0, b2 = 1): per voxel row of the tile, the lower

@@ -71,7 +71,8 @@ cudaError_t static_scratch(int device, void **out) {
 }
 
 struct StaticGeom {
-  int fw, fh, chunk_bp, chunk_fp;
+  int fw, fh, ffw, ffh, chunk_bp, chunk_fp;
+  float nbound;
   bool sep;
 };
 
@@ -81,7 +82,7 @@ struct StaticGeom {
 bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
             StaticGeom *out) {
   bool sep = true;
-  double span_u = 0, span_v = 0;
+  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
   const double two32 = 4294967296.0;
   const double ext = std::max(std::max(nx, ny), th) + 64.0;
   for (int t = 0; t < nt; ++t) {
@@ -100,17 +101,30 @@ bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
         fabs(k[4]) + (fabs(k[5]) + fabs(k[6]) + fabs(k[7])) * 2 * ext > 1.0e9)
       return false;
     if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
+    min_a1 = std::min(min_a1, fabs(k[1]));
     span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
                                   fabs(k[3]) * (kTZ - 1));
     span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
                                   fabs(k[7]) * (kTZ - 1));
+    fspan_u = std::max(fspan_u, fabs(k[1]) * (kFX - 1) + fabs(k[2]) * (kTY - 1) +
+                                    fabs(k[3]) * (kFTZ - 1));
+    fspan_v = std::max(fspan_v, fabs(k[5]) * (kFX - 1) + fabs(k[6]) * (kTY - 1) +
+                                    fabs(k[7]) * (kFTZ - 1));
   }
   out->fw = (int)ceil(span_u) + 4;
   out->fh = sep ? kTY : (int)ceil(span_v) + 5;
+  out->ffw = (int)ceil(fspan_u) + 4;
+  out->ffh = sep ? kTY : (int)ceil(fspan_v) + 5;
   out->sep = sep;
+  {
+    // forward-projection window bound, as the context path computes it
+    double bx = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
+    bx = std::min(bx, (double)kFX);
+    out->nbound = (float)(bx * kTY * kFTZ);
+  }
   const size_t ent_bp = (size_t)out->fw * out->fh * sizeof(float2);
-  const size_t ent_fp = (size_t)out->fw * out->fh * sizeof(float);
-  if (ent_bp > kStaticSmemMax) return false;
+  const size_t ent_fp = (size_t)out->ffw * out->ffh * sizeof(float);
+  if (ent_bp > kStaticSmemMax || ent_fp > kStaticSmemMax) return false;
   out->chunk_bp =
       (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemBp / ent_bp));
   out->chunk_fp =
@@ -167,9 +181,10 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   f.ox = ox;
   f.oy = oy;
   f.oz = oz;
-  f.fw = sg.fw;
-  f.fh = sg.fh;
+  f.fw = sg.ffw;
+  f.fh = sg.ffh;
   f.chunk = sg.chunk_fp;
+  f.nbound = sg.nbound;
 
   BpArgs bp;
   bp.v = v;

@@ -183,7 +183,9 @@ def test_zslabs_add_up(engine, restatement, layout):
     for z0, nz in ((0, 9), (9, th - 9)):
         view = v[:, z0:, :] if layout == 0 else v[z0:]
         engine.forward_project(view, summed, None, z0, nz)
-    assert O.rel_l2(host(summed), host(whole)) < 1e-6
+    # Slabs form different forward-projection tiles, hence different
+    # fixed-point scales (see test_cfg1_forward_projection_linear).
+    assert O.rel_l2(host(summed), host(whole)) < 2e-5
 
 
 @pytest.mark.parametrize("nx", [256, 1024, 4096])
