@@ -63,6 +63,7 @@ struct tr_ctx {
   float2 *ghat_d = nullptr, *tw_d = nullptr;
   float *hproj_d = nullptr, *hvol_d = nullptr;
   size_t hproj_n = 0, hvol_n = 0;
+  int *err_d = nullptr;  // [0] abort word of the current launch, [1] sticky report
 };
 
 namespace {
@@ -167,7 +168,30 @@ BpArgs bp_args(const tr_ctx *c, float *vol, int z0, int nz, const float *img,
   a.gamma = gamma;
   a.wtvol = nullptr;
   a.out = nullptr;
+  a.err = c->err_d;
   return a;
+}
+
+// Back-projection launch: clears the launch-wide abort word first.
+cudaError_t run_bp(tr_ctx *c, int mode, const BpArgs &a, cudaStream_t s) {
+  if (c->err_d) {
+    cudaError_t e = cudaMemsetAsync(c->err_d, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_bp(mode, c->sep, a, s);
+}
+
+// Reads and clears the sticky device-wait report (after a synchronisation).
+tr_status take_timeout(tr_ctx *c) {
+  if (!c->err_d) return TR_OK;
+  int h = 0;
+  if (cudaMemcpy(&h, c->err_d + 1, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return cuda_fail(c, cudaGetLastError(), "reading the device-wait flag");
+  if (!h) return TR_OK;
+  cudaMemset(c->err_d, 0, 2 * sizeof(int));
+  return fail(c, TR_ERR_TIMEOUT,
+              "a back-projection's staging copy did not arrive within its time limit; "
+              "the volume of that launch was left unchanged");
 }
 
 FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
@@ -377,7 +401,7 @@ tr_status ensure_wtvol(tr_ctx *c, cudaStream_t s) {
   if (!c->wtvol_ready) {
     BpArgs a = bp_args(c, c->wtvol_d, 0, c->th, nullptr, 0, c->nt, 1.f);
     a.out = c->wtvol_d;
-    TR_CUDA(c, launch_bp(BP_WEIGHTS, c->sep, a, s));
+    TR_CUDA(c, run_bp(c, BP_WEIGHTS, a, s));
     c->wtvol_ready = true;
   }
   return TR_OK;
@@ -454,6 +478,12 @@ tr_status tr_create(int device, size_t budget, tr_ctx **out) {
     delete c;
     return TR_ERR_CUDA;
   }
+  if (cudaMalloc(&c->err_d, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMemset(c->err_d, 0, 2 * sizeof(int)) != cudaSuccess) {
+    cudaStreamDestroy(c->io_stream);
+    delete c;
+    return TR_ERR_CUDA;
+  }
   *out = c;
   return TR_OK;
 }
@@ -468,6 +498,7 @@ tr_status tr_destroy(tr_ctx *c) {
   if (c->hproj_d) cudaFree(c->hproj_d);
   if (c->hvol_d) cudaFree(c->hvol_d);
   if (c->io_stream) cudaStreamDestroy(c->io_stream);
+  if (c->err_d) cudaFree(c->err_d);
   delete c;
   return TR_OK;
 }
@@ -539,7 +570,7 @@ tr_status tr_backproject(tr_ctx *c, const float *proj, float *vol, int z0, int n
   if (!proj || !vol || z0 < 0 || nz < 1 || z0 + nz > c->th)
     return fail(c, TR_ERR_ARG, "bad back-projection arguments (z0=%d nz=%d)", z0, nz);
   BpArgs a = bp_args(c, vol, z0, nz, proj, 0, c->nt, 1.f);
-  TR_CUDA(c, launch_bp(BP_NORM, c->sep, a, (cudaStream_t)stream));
+  TR_CUDA(c, run_bp(c, BP_NORM, a, (cudaStream_t)stream));
   return TR_OK;
 }
 
@@ -575,7 +606,7 @@ tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gam
     TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
     BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, 0, c->nt, gamma);
     b.wtvol = c->wtvol_d;
-    TR_CUDA(c, launch_bp(BP_SIRT, c->sep, b, s));
+    TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
   return TR_OK;
 }
@@ -599,7 +630,7 @@ tr_status tr_sart(tr_ctx *c, const float *proj, float *vol, int iters, float gam
       TR_CUDA(c, launch_fp(c->sep, f, s));
       TR_CUDA(c, launch_resid(proj + plane * t, vt, c->wt_d + plane * t, plane, c->nsm, s));
       BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, t, 1, gamma);
-      TR_CUDA(c, launch_bp(BP_NORM, c->sep, b, s));
+      TR_CUDA(c, run_bp(c, BP_NORM, b, s));
     }
   return TR_OK;
 }
@@ -643,14 +674,14 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   if (st) return st;
   TR_CUDA(c, cudaMemcpyAsync(vol_h, c->hvol_d, vn * sizeof(float), cudaMemcpyDeviceToHost, s));
   TR_CUDA(c, cudaStreamSynchronize(s));
-  return TR_OK;
+  return take_timeout(c);
 }
 
 tr_status tr_synchronize(tr_ctx *c) {
   if (!c) return TR_ERR_ARG;
   TR_CUDA(c, cudaSetDevice(c->device));
   TR_CUDA(c, cudaDeviceSynchronize());
-  return TR_OK;
+  return take_timeout(c);
 }
 
 }  // extern "C"

@@ -66,6 +66,12 @@ struct BpArgs {
   float gamma;
   const float *wtvol;  // BP_SIRT: per-voxel weight sums (same view strides)
   float *out;          // BP_WEIGHTS: output (same view strides)
+  int *err;            // err[0]: launch-wide abort word (zero at launch);
+                       // err[1]: sticky report word; both set to 1 when a
+                       // bounded device wait runs out.  nullptr: no TMA path.
+  // TMA staging (filled by the launcher): raw window box, raw buffer stride in
+  // floats and byte offset of the raw buffers in dynamic shared memory.
+  int tma_bw, tma_bh, tma_raw_stride, tma_raw_offset;
 };
 
 struct FpArgs {

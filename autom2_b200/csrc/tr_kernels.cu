@@ -31,6 +31,12 @@
 // any per-tilt y shift) interpolates in y with one weight per voxel row, so
 // the two rows are blended while staging and the inner loop is one table
 // read and one FMA per voxel and tilt.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <stdint.h>
+
+#include <algorithm>
+
 #include "tr_internal.cuh"
 
 namespace trb {
@@ -142,10 +148,89 @@ __device__ __forceinline__ float sep_at(const float *p, int nx, int ny,
   }
 }
 
+// Interpolation of one staged chunk of tilts into the thread's accumulators.
+template <int MODE, bool SEP>
+__device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], const void *tblv,
+                                              const TileTilt *tt, const TiltGeo *geo,
+                                              int nc, int per, int fw, int pny,
+                                              int lane, int wy, int wz) {
+  for (int i = 0; i < nc; ++i) {
+    const TiltGeo &g = geo[i];
+    const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
+    unsigned long long U = (unsigned long long)(tt[i].U0 + lane * A0 + wy * A1 +
+                                                (long long)(wz * kNV) * A2);
+    if (SEP) {
+      const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)(i * kTY + wy) * fw;
+#pragma unroll
+      for (int k = 0; k < kNV; ++k) {
+        const float2 t = T[(int)(U >> 32)];
+        acc[k] += fmaf(one_plus_frac(U), t.y, t.x);
+        U += (unsigned long long)A2;
+      }
+    } else {
+      const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
+      unsigned long long V = (unsigned long long)(tt[i].V0 + lane * B0 + wy * B1 +
+                                                  (long long)(wz * kNV) * B2);
+      const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)i * per;
+      const int jmin = tt[i].jmin;
+      if (MODE == BP_NORM && tt[i].check_rows) {
+#pragma unroll
+        for (int k = 0; k < kNV; ++k) {
+          const int q = (int)(U >> 32), r = (int)(V >> 32);
+          const float2 *e = T + r * fw + q;
+          const float2 t0 = e[0], t1 = e[fw];
+          const float f = one_plus_frac(U);
+          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
+          const float val = fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
+          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) acc[k] += val;
+          U += (unsigned long long)A2;
+          V += (unsigned long long)B2;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kNV; ++k) {
+          const int q = (int)(U >> 32), r = (int)(V >> 32);
+          const float2 *e = T + r * fw + q;
+          const float2 t0 = e[0], t1 = e[fw];
+          const float f = one_plus_frac(U);
+          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
+          acc[k] += fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
+          U += (unsigned long long)A2;
+          V += (unsigned long long)B2;
+        }
+      }
+    }
+  }
+}
+
+// Epilogue: one coalesced read-modify-write per voxel.
+template <int MODE>
+__device__ __forceinline__ void bp_epilogue(const BpArgs &a, const float (&acc)[kNV],
+                                            int x, int y, int zbase) {
+  if (x >= a.v.nx || y >= a.v.ny) return;
+#pragma unroll
+  for (int k = 0; k < kNV; ++k) {
+    const int z = zbase + k;
+    if (z >= a.v.nz) break;
+    const size_t idx = (size_t)y * a.v.sy + (size_t)z * a.v.sz + x;
+    if (MODE == BP_NORM) {
+      a.v.vol[idx] += a.gamma * acc[k];
+    } else if (MODE == BP_SIRT) {
+      const float w = a.wtvol[idx];
+      if (w != 0.f) a.v.vol[idx] += acc[k] / w * a.gamma;
+    } else {
+      a.out[idx] = acc[k];
+    }
+  }
+}
+
+// Back-projection with tables staged by the threads from global memory (any
+// image width; also the voxel-weight pass, which has no image).
 template <int MODE, bool SEP>
 __global__ void __launch_bounds__(kThreads)
     bp_kernel(const BpArgs a) {
-  extern __shared__ float2 tbl[];
+  extern __shared__ float4 tbl_raw[];
+  float2 *tbl2 = reinterpret_cast<float2 *>(tbl_raw);
   __shared__ TileTilt tt[kMaxChunk];
   __shared__ SepW sw[kMaxChunk][kTY];
 
@@ -179,80 +264,213 @@ __global__ void __launch_bounds__(kThreads)
       const float *p = a.img.p ? a.img.p + (size_t)(a.t0 + c0 + i) * a.img.tstride
                                : nullptr;
       const int x0 = tt[i].kmin + q;
-      float b, n;
       if (SEP) {
         const SepW s = sw[i][r];
         const bool valid = (MODE != BP_NORM) ||
                            ((s.w0 + s.w1) != 0.f && x0 >= -1 && x0 <= pnx - 1);
-        b = valid ? sep_at<MODE>(p, pnx, pny, s, x0) : 0.f;
-        n = valid ? sep_at<MODE>(p, pnx, pny, s, x0 + 1) : 0.f;
+        const float b = valid ? sep_at<MODE>(p, pnx, pny, s, x0) : 0.f;
+        const float n = valid ? sep_at<MODE>(p, pnx, pny, s, x0 + 1) : 0.f;
+        const float sl = n - b;
+        tbl2[e] = make_float2(b - sl, sl);
       } else {
         const int j = tt[i].jmin + r;
         const bool valid = (MODE != BP_NORM) ||
                            (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny);
-        b = valid ? img_at<MODE>(p, pnx, pny, j, x0) : 0.f;
-        n = valid ? img_at<MODE>(p, pnx, pny, j, x0 + 1) : 0.f;
+        const float b = valid ? img_at<MODE>(p, pnx, pny, j, x0) : 0.f;
+        const float n = valid ? img_at<MODE>(p, pnx, pny, j, x0 + 1) : 0.f;
+        const float sl = n - b;
+        tbl2[e] = make_float2(b - sl, sl);
       }
-      const float sl = n - b;
-      tbl[e] = make_float2(b - sl, sl);
     }
     __syncthreads();
+    bp_accumulate<MODE, SEP>(acc, tbl_raw, tt, a.geo + a.t0 + c0, nc, per, fw, pny, lane,
+                             wy, wz);
+    __syncthreads();
+  }
+  bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
+}
 
-    for (int i = 0; i < nc; ++i) {
-      const TiltGeo &g = a.geo[a.t0 + c0 + i];
-      const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
-      unsigned long long U = (unsigned long long)(tt[i].U0 + lane * A0 + wy * A1 +
-                                                  (long long)(wz * kNV) * A2);
+// ------------------------------------------------------------- TMA staging
+//
+// One elected thread issues, per tilt, a 3-D bulk tensor copy (TMA,
+// cp.async.bulk.tensor, no multicast) of the tile's raw detector window --
+// columns [kmin & ~3, +BW), rows [ys, +BH) of image `tilt` -- into a raw
+// shared buffer; the copies of the next chunk land while the CTA interpolates
+// the current one (two raw buffers, one mbarrier each).  TMA fills the parts
+// of a box outside the image with zeros.  The threads then turn the raw window
+// into interpolation-table entries with shared-memory reads only.  The global
+// tensor needs 16-byte row strides, so this path serves images whose width is
+// a multiple of 4; the others stage through bp_kernel.
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *m, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for a phase until it completes (true), `budget` clock cycles pass or
+// the launch-wide abort word becomes non-zero (false).
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *m, unsigned parity,
+                                                  long long budget, const int *abort_word) {
+  const long long t0 = clock64();
+  for (;;) {
+    if (mbar_try_wait(m, parity)) return true;
+    if (clock64() - t0 > budget) return false;
+    if (abort_word && *(volatile const int *)abort_word) return false;
+  }
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y,
+                                            int z, unsigned long long *m) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(m))
+      : "memory");
+}
+
+template <int MODE, bool SEP>
+__global__ void __launch_bounds__(kThreads)
+    bp_tma_kernel(const BpArgs a, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wy = (tid >> 5) % kTY;
+  const int wz = (tid >> 5) / kTY;
+  const int xc = blockIdx.x * kTX, yc = blockIdx.y * kTY, zl = blockIdx.z * kTZ;
+  const int zc = zl + a.v.zoff;
+  const int fw = a.fw, fh = SEP ? kTY : a.fh;
+  const int pnx = a.img.nx, pny = a.img.ny;
+  const int bw = a.tma_bw, bh = a.tma_bh, rs = a.tma_raw_stride;  // floats
+  const int nt = a.nt, chunk = a.chunk, per = fh * fw;
+
+  TileTilt *tt = reinterpret_cast<TileTilt *>(dsm);
+  SepW(*sw)[kTY] = reinterpret_cast<SepW(*)[kTY]>(dsm + (size_t)nt * sizeof(TileTilt));
+  float *raw0 = reinterpret_cast<float *>(dsm + a.tma_raw_offset);
+  float *tblf = raw0 + 2 * (size_t)chunk * rs;  // table entries (float2)
+  float2 *tbl2 = reinterpret_cast<float2 *>(tblf);
+
+  for (int i = tid; i < nt; i += kThreads) {
+    tile_setup(a.geo[a.t0 + i], xc, yc, zc, a.ox, a.oy, a.oz, pny, SEP, kTX - 1, kTY - 1,
+               kTZ - 1, tt[i], sw[i]);
+    if (SEP) {  // raw rows start at the lowest detector row of the tile
+      int y0 = sw[i][0].y0;
+      for (int r = 1; r < kTY; ++r) y0 = min(y0, sw[i][r].y0);
+      tt[i].jmin = y0;
+    }
+  }
+  if (tid == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+
+  const int nchunks = (nt + chunk - 1) / chunk;
+  auto issue = [&](int c, int buf) {
+    const int c0 = c * chunk, nc = min(chunk, nt - c0);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&mbar[buf], (unsigned)(nc * bw * bh * 4));
+    float *dst = raw0 + (size_t)buf * chunk * rs;
+    for (int i = 0; i < nc; ++i)
+      tma_load_3d(dst + (size_t)i * rs, &tmap, tt[c0 + i].kmin & ~3, tt[c0 + i].jmin,
+                  a.t0 + c0 + i, &mbar[buf]);
+  };
+  if (tid == 0) {
+    issue(0, 0);
+    if (nchunks > 1) issue(1, 1);
+  }
+
+  float acc[kNV];
+#pragma unroll
+  for (int k = 0; k < kNV; ++k) acc[k] = 0.f;
+
+  for (int c = 0; c < nchunks; ++c) {
+    const int buf = c & 1, c0 = c * chunk, nc = min(chunk, nt - c0);
+    // ~1 s budget for a copy; a CTA that gives up raises the launch-wide
+    // abort word (err[0]) and the sticky report word (err[1]) so that the
+    // other CTAs stop waiting too.
+    const bool ok = mbar_wait_bounded(&mbar[buf], (unsigned)((c >> 1) & 1), 1ll << 31, a.err);
+    if (__syncthreads_or(!ok)) {
+      // Report, give the copies this CTA still has in flight a bounded
+      // chance to land, and leave the volume untouched.
+      if (tid == 0) {
+        atomicExch(a.err, 1);
+        atomicExch(a.err + 1, 1);
+      }
+      mbar_wait_bounded(&mbar[buf], (unsigned)((c >> 1) & 1), 1ll << 28, nullptr);
+      if (c + 1 < nchunks)
+        mbar_wait_bounded(&mbar[buf ^ 1], (unsigned)(((c + 1) >> 1) & 1), 1ll << 28, nullptr);
+      return;
+    }
+    const float *R0 = raw0 + (size_t)buf * chunk * rs;
+    for (int e = tid; e < nc * per; e += kThreads) {
+      const int i = e / per, rq = e - i * per;
+      const int r = rq / fw, q = rq - r * fw;
+      const TileTilt &t = tt[c0 + i];
+      if (r >= t.nr || q >= t.nq) continue;
+      const float *R = R0 + (size_t)i * rs;
+      const int xs = t.kmin & ~3, ys = t.jmin;
+      const int x0 = t.kmin + q;
       if (SEP) {
-        const float2 *T = tbl + (size_t)(i * kTY + wy) * fw;
-#pragma unroll
-        for (int k = 0; k < kNV; ++k) {
-          const float2 t = T[(int)(U >> 32)];
-          acc[k] += fmaf(one_plus_frac(U), t.y, t.x);
-          U += (unsigned long long)A2;
+        const SepW s = sw[c0 + i][r];
+        const float *r0 = R + (s.y0 - ys) * bw - xs, *r1 = r0 + bw;
+        float b = 0.f, n = 0.f;
+        if (MODE == BP_NORM) {
+          if ((s.w0 + s.w1) != 0.f && x0 >= -1 && x0 <= pnx - 1) {
+            const int kb = clampi(x0, 0, pnx - 1), kn = clampi(x0 + 1, 0, pnx - 1);
+            const float c = s.w0 + s.w1;
+            b = (s.w0 * (s.w0 != 0.f ? r0[kb] : 0.f) + s.w1 * (s.w1 != 0.f ? r1[kb] : 0.f)) / c;
+            n = (s.w0 * (s.w0 != 0.f ? r0[kn] : 0.f) + s.w1 * (s.w1 != 0.f ? r1[kn] : 0.f)) / c;
+          }
+        } else {
+          b = s.w0 * r0[x0] + s.w1 * r1[x0];
+          n = s.w0 * r0[x0 + 1] + s.w1 * r1[x0 + 1];
         }
+        const float sl = n - b;
+        tbl2[e] = make_float2(b - sl, sl);
       } else {
-        const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
-        unsigned long long V = (unsigned long long)(tt[i].V0 + lane * B0 + wy * B1 +
-                                                    (long long)(wz * kNV) * B2);
-        const float2 *T = tbl + (size_t)i * per;
-        const bool chk = (MODE == BP_NORM) && tt[i].check_rows;
-        const int jmin = tt[i].jmin;
-#pragma unroll
-        for (int k = 0; k < kNV; ++k) {
-          const int q = (int)(U >> 32), r = (int)(V >> 32);
-          const float2 *e = T + r * fw + q;
-          const float2 t0 = e[0], t1 = e[fw];
-          const float f = one_plus_frac(U);
-          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          float val = fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
-          if (chk && (unsigned)(jmin + r + 1) > (unsigned)pny) val = 0.f;
-          acc[k] += val;
-          U += (unsigned long long)A2;
-          V += (unsigned long long)B2;
+        const int j = ys + r;
+        float b = 0.f, n = 0.f;
+        if (MODE == BP_NORM) {
+          if (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny) {
+            const float *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
+            b = row[clampi(x0, 0, pnx - 1)];
+            n = row[clampi(x0 + 1, 0, pnx - 1)];
+          }
+        } else {
+          const float *row = R + r * bw - xs;
+          b = row[x0];
+          n = row[x0 + 1];
         }
+        const float sl = n - b;
+        tbl2[e] = make_float2(b - sl, sl);
       }
     }
     __syncthreads();
+    if (tid == 0 && c + 2 < nchunks) issue(c + 2, buf);
+    bp_accumulate<MODE, SEP>(acc, tblf, tt + c0, a.geo + a.t0 + c0, nc, per, fw, pny, lane,
+                             wy, wz);
+    __syncthreads();
   }
-
-  // Epilogue: one coalesced read-modify-write per voxel.
-  const int x = xc + lane, y = yc + wy;
-  if (x >= a.v.nx || y >= a.v.ny) return;
-#pragma unroll
-  for (int k = 0; k < kNV; ++k) {
-    const int z = zl + wz * kNV + k;
-    if (z >= a.v.nz) break;
-    const size_t idx = (size_t)y * a.v.sy + (size_t)z * a.v.sz + x;
-    if (MODE == BP_NORM) {
-      a.v.vol[idx] += a.gamma * acc[k];
-    } else if (MODE == BP_SIRT) {
-      const float w = a.wtvol[idx];
-      if (w != 0.f) a.v.vol[idx] += acc[k] / w * a.gamma;
-    } else {
-      a.out[idx] = acc[k];
-    }
-  }
+  bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
 }
 
 // Forward projection: voxel splat (Reproject, main/main-mpi.cpp:286-344) of
@@ -260,9 +478,9 @@ __global__ void __launch_bounds__(kThreads)
 // touched in-image detector pixel.  v.vol == nullptr splats ones (the
 // per-pixel weight sums, reproj_wt).
 //
-// Each lane owns the voxel pair (x, x+1) with x = xc + 2*lane.  Their columns
-// are q and q or q+1 (the x slope is at most 1), so the pair's splat folds
-// into three columns per detector row in registers.
+// Each lane owns the voxel pair (x, x+1) with x = xc + 2*lane and splats
+// the two voxels in turn: lanes of one atomic instruction are then two voxels
+// apart along x and land on distinct detector columns whenever |a1| >= 0.5.
 //
 // The windows accumulate in 32-bit fixed point with native shared-memory
 // integer atomics (fire-and-forget; float atomics on shared memory are a
@@ -309,6 +527,7 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
   // Tile scale: largest |v| over the tile (as ordered float bits).
   __shared__ unsigned wmax[kThreads / 32];
   __shared__ float s_scale, s_inv;
+  __shared__ int s_nonzero;
   {
     unsigned m = 0;
 #pragma unroll
@@ -327,6 +546,7 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
       frexpf(lim, &ex);  // lim = m 2^ex, m in [0.5, 1): 2^(ex-1) <= lim
       s_scale = ldexpf(1.f, ex - 1);
       s_inv = ldexpf(1.f, 1 - ex);
+      s_nonzero = vmax > 0.f;
     }
     __syncthreads();
     const float S = s_scale;
@@ -337,6 +557,7 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
     }
   }
   int *const iacc = reinterpret_cast<int *>(accs);
+  const bool s_scale_nonzero = s_nonzero != 0;  // an all-zero tile adds nothing
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
@@ -346,88 +567,65 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
     for (int e = tid; e < nc * per; e += kThreads) iacc[e] = 0;
     __syncthreads();
 
-    for (int i = 0; i < nc; ++i) {
+    for (int i = 0; i < nc && s_scale_nonzero; ++i) {
       const TiltGeo &g = a.geo[a.t0 + c0 + i];
       const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
-      unsigned long long U = (unsigned long long)(tt[i].U0 + (2 * lane) * A0 +
-                                                  wy * A1 + (long long)(wz * kFNV) * A2);
+      // Lane coordinates of the pair's voxels: A at x = xc + 2 lane, B at x+1.
+      unsigned long long UA = (unsigned long long)(tt[i].U0 + (2 * lane) * A0 +
+                                                   wy * A1 + (long long)(wz * kFNV) * A2);
+      unsigned long long UB = UA + (unsigned long long)A0;
       if (SEP) {
         int *T = iacc + (size_t)(i * kTY + wy) * fw;
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
+          // dx*v as one rounding of (1+dx)*v - v; the pair's lanes are two x
+          // apart, so one instruction's lanes hit distinct columns.
           const float vA = va[k], vB = vb[k];
-          if (vA != 0.f || vB != 0.f) {
-            const unsigned long long UB = U + (unsigned long long)A0;
-            const int qa = (int)(U >> 32), qb = (int)(UB >> 32);
-            const float dxa = one_plus_frac(U) - 1.f, dxb = one_plus_frac(UB) - 1.f;
-            const float t1a = dxa * vA, t0a = vA - t1a;
-            const float t1b = dxb * vB, t0b = vB - t1b;
-            int *e = T + qa;
-            if (qb == qa) {
-              wadd(e, t0a + t0b);
-              wadd(e + 1, t1a + t1b);
-            } else if (qb == qa + 1) {
-              wadd(e, t0a);
-              wadd(e + 1, t1a + t0b);
-              wadd(e + 2, t1b);
-            } else {
-              wadd(e, t0a);
-              wadd(e + 1, t1a);
-              int *f = T + qb;
-              wadd(f, t0b);
-              wadd(f + 1, t1b);
-            }
-          }
-          U += (unsigned long long)A2;
+          const float t1a = fmaf(one_plus_frac(UA), vA, -vA), t0a = vA - t1a;
+          const float t1b = fmaf(one_plus_frac(UB), vB, -vB), t0b = vB - t1b;
+          int *ea = T + (int)(UA >> 32), *eb = T + (int)(UB >> 32);
+          wadd(ea, t0a);
+          wadd(ea + 1, t1a);
+          wadd(eb, t0b);
+          wadd(eb + 1, t1b);
+          UA += (unsigned long long)A2;
+          UB += (unsigned long long)A2;
         }
       } else {
         const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
-        unsigned long long V = (unsigned long long)(tt[i].V0 + (2 * lane) * B0 +
-                                                    wy * B1 + (long long)(wz * kFNV) * B2);
+        unsigned long long VA = (unsigned long long)(tt[i].V0 + (2 * lane) * B0 +
+                                                     wy * B1 + (long long)(wz * kFNV) * B2);
+        unsigned long long VB = VA + (unsigned long long)B0;
         int *T = iacc + (size_t)i * per;
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
           const float vA = va[k], vB = vb[k];
-          if (vA != 0.f || vB != 0.f) {
-            const unsigned long long UB = U + (unsigned long long)A0;
-            const unsigned long long VB = V + (unsigned long long)B0;
-            const int qa = (int)(U >> 32), qb = (int)(UB >> 32);
-            const int ra = (int)(V >> 32), rb = (int)(VB >> 32);
-            const float dxa = one_plus_frac(U) - 1.f, dya = one_plus_frac(V) - 1.f;
-            const float dxb = one_plus_frac(UB) - 1.f, dyb = one_plus_frac(VB) - 1.f;
-            const float ya1 = dya * vA, ya0 = vA - ya1;
-            const float a01 = dxa * ya0, a00 = ya0 - a01;
-            const float a11 = dxa * ya1, a10 = ya1 - a11;
-            const float yb1 = dyb * vB, yb0 = vB - yb1;
-            const float b01 = dxb * yb0, b00 = yb0 - b01;
-            const float b11 = dxb * yb1, b10 = yb1 - b11;
-            int *e = T + ra * fw + qa;
-            if (rb == ra && qb == qa) {
-              wadd(e, a00 + b00);
-              wadd(e + 1, a01 + b01);
-              wadd(e + fw, a10 + b10);
-              wadd(e + fw + 1, a11 + b11);
-            } else if (rb == ra && qb == qa + 1) {
-              wadd(e, a00);
-              wadd(e + 1, a01 + b00);
-              wadd(e + 2, b01);
-              wadd(e + fw, a10);
-              wadd(e + fw + 1, a11 + b10);
-              wadd(e + fw + 2, b11);
-            } else {
-              wadd(e, a00);
-              wadd(e + 1, a01);
-              wadd(e + fw, a10);
-              wadd(e + fw + 1, a11);
-              int *f = T + rb * fw + qb;
-              wadd(f, b00);
-              wadd(f + 1, b01);
-              wadd(f + fw, b10);
-              wadd(f + fw + 1, b11);
-            }
+          {
+            const float y1 = fmaf(one_plus_frac(VA), vA, -vA), y0 = vA - y1;
+            const float fx = one_plus_frac(UA);
+            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
+            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            int *e = T + (int)(VA >> 32) * fw + (int)(UA >> 32);
+            wadd(e, t00);
+            wadd(e + 1, t01);
+            wadd(e + fw, t10);
+            wadd(e + fw + 1, t11);
           }
-          U += (unsigned long long)A2;
-          V += (unsigned long long)B2;
+          {
+            const float y1 = fmaf(one_plus_frac(VB), vB, -vB), y0 = vB - y1;
+            const float fx = one_plus_frac(UB);
+            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
+            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            int *e = T + (int)(VB >> 32) * fw + (int)(UB >> 32);
+            wadd(e, t00);
+            wadd(e + 1, t01);
+            wadd(e + fw, t10);
+            wadd(e + fw + 1, t11);
+          }
+          UA += (unsigned long long)A2;
+          UB += (unsigned long long)A2;
+          VA += (unsigned long long)B2;
+          VB += (unsigned long long)B2;
         }
       }
     }
@@ -494,15 +692,92 @@ static cudaError_t launch_bp_t(const BpArgs &a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+constexpr size_t kSmemTma = 56 * 1024;
+
+// TMA-staged launch; returns false (nothing launched) when the image or the
+// window does not fit the TMA path.
+template <int MODE, bool SEP>
+static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err) {
+  const ImgView &im = a0.img;
+  if (!im.p || !a0.err || im.nx % 4 != 0 || (reinterpret_cast<uintptr_t>(im.p) & 15) != 0)
+    return false;
+  const int fh = SEP ? kTY : a0.fh;
+  const int bw = (a0.fw + 4 + 3) & ~3;
+  const int bh = SEP ? kTY + 3 : fh + 1;
+  if (bw > 256 || bh > 256) return false;
+  const int rs = (bw * bh + 31) & ~31;  // floats; 128-byte aligned raw slots
+  const size_t fixed =
+      ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
+  const size_t per_tilt = 2 * (size_t)rs * 4 + (size_t)fh * a0.fw * sizeof(float2);
+  if (fixed + per_tilt > kSmemTma + 64 * 1024) return false;
+  int chunk = (int)std::max<size_t>(1, (kSmemTma > fixed ? kSmemTma - fixed : 0) / per_tilt);
+  chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
+  const size_t smem = fixed + (size_t)chunk * per_tilt;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return false;
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {(cuuint64_t)im.nx, (cuuint64_t)im.ny,
+                              (cuuint64_t)(a0.t0 + a0.nt)};
+  const cuuint64_t strides[2] = {(cuuint64_t)im.nx * 4, (cuuint64_t)im.tstride * 4};
+  const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(im.p), dims, strides,
+          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  BpArgs a = a0;
+  a.chunk = chunk;
+  a.tma_bw = bw;
+  a.tma_bh = bh;
+  a.tma_raw_stride = rs;
+  a.tma_raw_offset = (int)fixed;
+  cudaError_t e = cudaFuncSetAttribute(bp_tma_kernel<MODE, SEP>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) {
+    bp_tma_kernel<MODE, SEP><<<tile_grid(a.v), kThreads, smem, s>>>(a, map);
+    e = cudaGetLastError();
+  }
+  *err = e;
+  return true;
+}
+
+template <int MODE, bool SEP>
+static cudaError_t launch_bp_any(const BpArgs &a, cudaStream_t s) {
+  if (MODE != BP_WEIGHTS) {
+    cudaError_t e;
+    if (try_launch_bp_tma<MODE, SEP>(a, s, &e)) return e;
+  }
+  return launch_bp_t<MODE, SEP>(a, s);
+}
+
 cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s) {
   if (sep) {
-    if (mode == BP_NORM) return launch_bp_t<BP_NORM, true>(a, s);
-    if (mode == BP_SIRT) return launch_bp_t<BP_SIRT, true>(a, s);
-    return launch_bp_t<BP_WEIGHTS, true>(a, s);
+    if (mode == BP_NORM) return launch_bp_any<BP_NORM, true>(a, s);
+    if (mode == BP_SIRT) return launch_bp_any<BP_SIRT, true>(a, s);
+    return launch_bp_any<BP_WEIGHTS, true>(a, s);
   }
-  if (mode == BP_NORM) return launch_bp_t<BP_NORM, false>(a, s);
-  if (mode == BP_SIRT) return launch_bp_t<BP_SIRT, false>(a, s);
-  return launch_bp_t<BP_WEIGHTS, false>(a, s);
+  if (mode == BP_NORM) return launch_bp_any<BP_NORM, false>(a, s);
+  if (mode == BP_SIRT) return launch_bp_any<BP_SIRT, false>(a, s);
+  return launch_bp_any<BP_WEIGHTS, false>(a, s);
 }
 
 static dim3 fp_grid(const VolView &v) {

@@ -137,10 +137,11 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
               const float *proj, float *vol, int iters, float gamma,
               cudaStream_t s) {
   const size_t plane = (size_t)nx * ny * nt, nvox = (size_t)nx * ny * th;
+  const size_t flag_b = 256;  // device-wait words of the back-projections
   const size_t geo_b = round256(sizeof(TiltGeo) * nt);
   const size_t plane_b = round256(plane * sizeof(float));
   const size_t vox_b = round256(nvox * sizeof(float));
-  if (geo_b + 2 * plane_b + vox_b > kStaticScratchBytes) return TR_ERR_BUDGET;
+  if (flag_b + geo_b + 2 * plane_b + vox_b > kStaticScratchBytes) return TR_ERR_BUDGET;
 
   TiltGeo g[kStaticMaxTilts];
   StaticGeom sg;
@@ -148,7 +149,8 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
 
   void *base = nullptr;
   if (static_scratch(device, &base) != cudaSuccess) return TR_ERR_CUDA;
-  unsigned char *b = (unsigned char *)base;
+  int *flags = (int *)base;
+  unsigned char *b = (unsigned char *)base + flag_b;
   TiltGeo *geo = (TiltGeo *)b;
   float *wt = (float *)(b + geo_b);
   float *val = (float *)(b + geo_b + plane_b);
@@ -201,6 +203,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   bp.fh = sg.fh;
   bp.chunk = sg.chunk_bp;
   bp.wtvol = wtvol;
+  bp.err = flags;
 
   // Geometry-only weights: splat of ones (projection side) and Σ_t c_t
   // (voxel side); the previous call's contents are cleared first.
@@ -214,6 +217,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   bw.img.p = nullptr;
   bw.gamma = 1.f;
   bw.out = wtvol;
+  if (cudaMemsetAsync(flags, 0, 2 * sizeof(int), s) != cudaSuccess) return TR_ERR_CUDA;
   if (launch_bp(BP_WEIGHTS, sg.sep, bw, s) != cudaSuccess) return TR_ERR_CUDA;
 
   for (int it = 0; it < iters; ++it) {
@@ -227,6 +231,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
     bi.img.p = val;
     bi.gamma = gamma;
     bi.out = nullptr;
+    if (cudaMemsetAsync(flags, 0, sizeof(int), s) != cudaSuccess) return TR_ERR_CUDA;
     if (launch_bp(BP_SIRT, sg.sep, bi, s) != cudaSuccess) return TR_ERR_CUDA;
   }
   return TR_OK;
