@@ -1,0 +1,166 @@
+"""The drop-in executables against the reference's own executables (GPU).
+
+The reference TiltRec-mpi / TiltRecZ-mpi are the unmodified reference sources
+built into oracle/_ref (one rank).  Both sides read the same MRC stack and
+tilt file; the output headers must match field for field (the statistics to
+float tolerance) and the volumes to relative L2 1e-5.  TiltRecZ-mpi's BPT and
+SIRT abort before writing their output (a double free in the reference), so
+those two are checked against the oracle restatement instead."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle as O
+from autom2_b200 import build
+from autom2_b200 import tiltrec as T
+from mrc_util import read_mrc, write_angles, write_mrc
+
+pytestmark = pytest.mark.gpu
+BIN = os.path.join(os.path.dirname(build.LIB), "..", "bin")
+TOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def case(tmp_path_factory):
+    build.build()
+    d = tmp_path_factory.mktemp("cli")
+    rng = np.random.default_rng(3)
+    nx, ny, nt = 64, 40, 13
+    ang = np.linspace(-60, 60, nt).astype(np.float32)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    write_mrc(d / "stack.mrc", proj)
+    write_angles(d / "a.rawtlt", ang)
+    return d, proj, ang
+
+
+def ours(layout, *args):
+    exe = os.path.join(BIN, "TiltRec-cuda" if layout == 0 else "TiltRecZ-cuda")
+    r = subprocess.run([exe, *args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr + r.stdout
+    return r
+
+
+def reference(layout, *args):
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    exe = os.path.join(O.REF_DIR, "TiltRec-mpi" if layout == 0 else "TiltRecZ-mpi")
+    r = subprocess.run([exe, *args], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return r
+
+
+def compare(a_path, b_path, tol=TOL, sections=None):
+    ha, ra, da = read_mrc(a_path)
+    hb, rb, db = read_mrc(b_path)
+    if sections is not None:
+        da, db = da[sections], db[sections]
+    for f in ("nx", "ny", "nz", "mode", "m", "len", "ang", "map", "next", "creatid", "nlabl"):
+        assert np.array_equal(ha[f], hb[f]), f
+    # everything outside the statistics is byte-identical
+    strip = lambda r: r[:76] + r[88:]  # noqa: E731  (amin/amax/amean at bytes 76..87)
+    assert strip(ra) == strip(rb)
+    for f in ("amin", "amax", "amean"):
+        assert abs(float(ha[f]) - float(hb[f])) <= 1e-4 * max(1.0, abs(float(hb[f]))), f
+    assert O.rel_l2(da, db) < tol
+
+
+@pytest.mark.parametrize("method", ["BPT", "WBP", "SIRT,3,0.5", "SART,1,0.4"])
+@pytest.mark.parametrize("geometry", ["0,0,0,12", "1.5,2.0,-1.5,10"])
+def test_tiltrec_vs_tiltrec_mpi(case, method, geometry):
+    d, proj, ang = case
+    a, b = d / f"ours_{method}_{geometry}.mrc", d / f"ref_{method}_{geometry}.mrc"
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", geometry, "--method", method]
+    ours(0, *common, "--output", str(a))
+    reference(0, *common, "--output", str(b))
+    # With XTILT != 0 a single TiltRec-mpi rank keeps add_right =
+    # ceil(|tan(pitch)| * thickness) (main-mpi.cpp:728-740: the first branch
+    # resets only add_left), so it reads that many rows past the end of the
+    # stack (unread, uninitialised) and reconstructs them into the top
+    # sections.  Those sections are excluded; the rest must match.
+    pitch = float(geometry.split(",")[1])
+    cut = slice(0, proj.shape[1] - 2) if pitch else None
+    compare(a, b, sections=cut)
+
+
+def test_initial_volume(case):
+    d, proj, ang = case
+    th = 8
+    init = np.random.default_rng(9).normal(size=(40, th, 64)).astype(np.float32)
+    write_mrc(d / "init.mrc", init)
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", f"0,0,0,{th}", "--method", "SIRT,2,0.5"]
+    ours(0, *common, "--output", str(d / "oi.mrc"), "--initial", str(d / "init.mrc"))
+    reference(0, *common, "--output", str(d / "ri.mrc"), "--initial", str(d / "init.mrc"))
+    compare(d / "oi.mrc", d / "ri.mrc")
+
+
+@pytest.mark.parametrize("method", ["WBP", "SART,1,0.4"])
+def test_tiltrecz_vs_tiltrecz_mpi(case, method):
+    d, proj, ang = case
+    a, b = d / f"oz_{method}.mrc", d / f"rz_{method}.mrc"
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", "1.0,0,2.0,12", "--method", method]
+    ours(1, *common, "--output", str(a))
+    reference(1, *common, "--output", str(b))
+    compare(a, b)
+
+
+@pytest.mark.parametrize("method,iters", [("BPT", 0), ("SIRT", 2)])
+def test_tiltrecz_vs_oracle(case, restatement, method, iters):
+    d, proj, ang = case
+    nt, ny, nx = proj.shape
+    th = 12
+    out = d / f"oz_{method}.mrc"
+    m = method if not iters else f"{method},{iters},0.6"
+    ours(1, "--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+         "--geometry", f"1.0,0,2.0,{th}", "--method", m, "--output", str(out))
+    c8 = restatement.coeffs(ang, 1.0, 0.0, 2.0)
+    org = T.default_origin(T.LAYOUT_Z, nx, ny, th)
+    g = restatement.geom(nx, ny, nt, th, 1, 0, org)
+    zero = np.zeros((th, ny, nx), np.float32)
+    want = (restatement.backproject(g, c8, proj, zero) if method == "BPT"
+            else restatement.sirt(g, c8, proj, zero, iters, 0.6))
+    _, _, got = read_mrc(out)
+    assert O.rel_l2(got, want) < TOL
+
+
+def test_byte_and_short_stacks(case, restatement):
+    d, proj, ang = case
+    q = np.clip(np.round(proj * 20), -120, 120)
+    for mode in (0, 1):
+        write_mrc(d / f"stack{mode}.mrc", q, mode=mode, next_bytes=64 if mode else 0)
+        common = ["--input", str(d / f"stack{mode}.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+                  "--geometry", "0,0,0,8", "--method", "BPT"]
+        ours(0, *common, "--output", str(d / f"ob{mode}.mrc"))
+        reference(0, *common, "--output", str(d / f"rb{mode}.mrc"))
+        compare(d / f"ob{mode}.mrc", d / f"rb{mode}.mrc")
+
+
+def test_f2b_bytes(case):
+    """--f2b: 64-row slabs, EMA mean/deviation (alpha 0.9), z-score clamped
+    to +-10 and mapped to 0..255 (recon_y.cu:164-181, basic.cu:442-475)."""
+    d, proj, ang = case
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", "0,0,0,8", "--method", "BPT"]
+    ours(0, *common, "--output", str(d / "of.mrc"))
+    ours(0, *common, "--output", str(d / "ob.mrc"), "--f2b")
+    _, _, vol = read_mrc(d / "of.mrc")
+    hb, _, got = read_mrc(d / "ob.mrc")
+    assert int(hb["mode"]) == 0
+    flat = vol.reshape(-1).astype(np.float32)
+    slab = 64 * 8 * 64
+    want = np.zeros(flat.size, np.uint8)
+    gm = gs = np.float32(0)
+    for s0 in range(0, flat.size, slab):
+        c = flat[s0:s0 + slab]
+        m = np.float32(c.astype(np.float64).mean())
+        sd = np.float32(np.sqrt(np.float32(((c - m).astype(np.float64) ** 2).mean())))
+        gm = np.float32(0.9) * gm + np.float32(0.1) * m
+        gs = np.float32(0.9) * gs + np.float32(0.1) * sd
+        n4 = (c.size // 4) * 4
+        z = np.clip((c[:n4] - gm) / gs, -10, 10)
+        want[s0:s0 + n4] = (((z + 10) / 20) * 255).astype(np.uint8)
+    assert np.mean(np.abs(got.reshape(-1).astype(int) - want.astype(int)) <= 1) > 0.999
