@@ -19,6 +19,11 @@ cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
 cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
 cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
                          int nsm, cudaStream_t s);
+cudaError_t launch_quantize(const float *p, size_t plane, int nt, int dtype, void *out,
+                            float *scale, unsigned *maxbits, int nsm, cudaStream_t s);
+cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const float *val,
+                            const float *wt, size_t plane, int nt, int rdtype, void *r,
+                            const float *rs, int nsm, cudaStream_t s);
 struct FilterArgs {
   float *rows;
   long long nrows;
@@ -58,6 +63,8 @@ struct tr_ctx {
   // scratch
   size_t scratch = 0;
   float *val_d = nullptr, *wt_d = nullptr, *wtvol_d = nullptr;
+  void *res16_d = nullptr;      // 16-bit SIRT residual [ntilt][ny][nx]
+  unsigned *maxbits_d = nullptr;  // per-tilt |p| maxima for tr_quantize
   bool wt_ready = false, wtvol_ready = false;
   int filt_nx = 0, filt_npad = 0, filt_log2m = 0;
   float2 *ghat_d = nullptr, *tw_d = nullptr;
@@ -123,6 +130,8 @@ void release_problem(tr_ctx *c) {
   scratch_free(c, (void **)&c->val_d, pb);
   scratch_free(c, (void **)&c->wt_d, pb);
   scratch_free(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float));
+  scratch_free(c, (void **)&c->res16_d, proj_elems(c) * 2);
+  scratch_free(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt);
   if (c->geo_d) {
     cudaFree(c->geo_d);
     c->geo_d = nullptr;
@@ -156,6 +165,8 @@ BpArgs bp_args(const tr_ctx *c, float *vol, int z0, int nz, const float *img,
   a.img.nx = c->nx;
   a.img.ny = c->ny;
   a.img.tstride = (long long)c->nx * c->ny;
+  a.img.dtype = IMG_F32;
+  a.img.scale = nullptr;
   a.geo = c->geo_d;
   a.t0 = t0;
   a.nt = nt;
@@ -632,6 +643,72 @@ tr_status tr_sart(tr_ctx *c, const float *proj, float *vol, int iters, float gam
       BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, t, 1, gamma);
       TR_CUDA(c, run_bp(c, BP_NORM, b, s));
     }
+  return TR_OK;
+}
+
+tr_status tr_quantize(tr_ctx *c, const float *proj, int dtype, void *out, float *scale,
+                      void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !out || !scale || (dtype != TR_DTYPE_F16 && dtype != TR_DTYPE_BF16))
+    return fail(c, TR_ERR_ARG, "bad quantize arguments (dtype=%d)", dtype);
+  if ((st = scratch_alloc(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt,
+                          "per-tilt maxima")))
+    return st;
+  TR_CUDA(c, launch_quantize(proj, (size_t)c->nx * c->ny, c->nt, dtype, out, scale,
+                             c->maxbits_d, c->nsm, (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_backproject_lp(tr_ctx *c, const void *proj, int dtype, const float *scale,
+                            float *vol, int z0, int nz, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || z0 < 0 || nz < 1 || z0 + nz > c->th ||
+      (dtype != TR_DTYPE_F32 && dtype != TR_DTYPE_F16 && dtype != TR_DTYPE_BF16))
+    return fail(c, TR_ERR_ARG, "bad back-projection arguments (z0=%d nz=%d dtype=%d)", z0,
+                nz, dtype);
+  BpArgs a = bp_args(c, vol, z0, nz, (const float *)proj, 0, c->nt, 1.f);
+  a.img.dtype = dtype;
+  a.img.scale = scale;
+  TR_CUDA(c, run_bp(c, BP_NORM, a, (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale, int rdtype,
+                     float *vol, int iters, float gamma, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  auto ok_dtype = [](int d) {
+    return d == TR_DTYPE_F32 || d == TR_DTYPE_F16 || d == TR_DTYPE_BF16;
+  };
+  if (!proj || !vol || iters < 0 || !ok_dtype(pdtype) || !ok_dtype(rdtype) ||
+      (pdtype != TR_DTYPE_F32 && !scale) || (rdtype == TR_DTYPE_F16 && !scale))
+    return fail(c, TR_ERR_ARG, "bad SIRT arguments (proj dtype %d, residual dtype %d)",
+                pdtype, rdtype);
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t plane = (size_t)c->nx * c->ny, pn = proj_elems(c);
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection"))) return st;
+  if (rdtype != TR_DTYPE_F32 &&
+      (st = scratch_alloc(c, &c->res16_d, pn * 2, "16-bit residual")))
+    return st;
+  if ((st = ensure_wt(c, s))) return st;
+  if ((st = ensure_wtvol(c, s))) return st;
+  const float *ps = pdtype == TR_DTYPE_F32 ? nullptr : scale;
+  const float *rs = rdtype == TR_DTYPE_F16 ? scale : nullptr;
+  void *res = rdtype == TR_DTYPE_F32 ? (void *)c->val_d : c->res16_d;
+  for (int it = 0; it < iters; ++it) {
+    TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
+    FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
+    TR_CUDA(c, launch_fp(c->sep, f, s));
+    TR_CUDA(c, launch_resid_lp(proj, pdtype, ps, c->val_d, c->wt_d, plane, c->nt, rdtype, res,
+                               rs, c->nsm, s));
+    BpArgs b = bp_args(c, vol, 0, c->th, (const float *)res, 0, c->nt, gamma);
+    b.img.dtype = rdtype;
+    b.img.scale = rs;
+    b.wtvol = c->wtvol_d;
+    TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
+  }
   return TR_OK;
 }
 

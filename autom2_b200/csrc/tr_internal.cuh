@@ -43,11 +43,15 @@ struct VolView {
   int zoff;
 };
 
-// Projection images [tilt][ny][nx].
+// Projection images [tilt][ny][nx].  dtype: IMG_F32 / IMG_F16 / IMG_BF16
+// elements; value = element * scale[tilt] (scale == nullptr: 1).
+enum { IMG_F32 = 0, IMG_F16 = 1, IMG_BF16 = 2 };
 struct ImgView {
-  const float *p;
+  const float *p;  // element pointer, reinterpreted per dtype
   int nx, ny;
   long long tstride;
+  int dtype;
+  const float *scale;
 };
 
 enum BpMode {

@@ -33,7 +33,11 @@
 // read and one FMA per voxel and tilt.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include <algorithm>
 
@@ -45,6 +49,11 @@ __device__ __forceinline__ float one_plus_frac(unsigned long long U) {
   // 1 + (low 32 bits / 2^32), truncated to the 23-bit float mantissa.
   return __uint_as_float(0x3F800000u | ((unsigned)U >> 9));
 }
+
+// Image element -> float.
+__device__ __forceinline__ float to_f(float v) { return v; }
+__device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 // Adds the scaled contribution x (|x| <= 2^21) to a fixed-point window entry,
 // rounded to the nearest integer by the 1.5*2^23 float shift.
@@ -117,40 +126,55 @@ __device__ void tile_setup(const TiltGeo &g, int xc, int yc, int zc, float ox,
 
 // Image value for table staging.  MODE: BP_NORM clamped, BP_SIRT zero padded,
 // BP_WEIGHTS indicator.
-template <int MODE>
-__device__ __forceinline__ float img_at(const float *p, int nx, int ny, int j,
+template <int MODE, typename IT>
+__device__ __forceinline__ float img_at(const IT *p, float sc, int nx, int ny, int j,
                                         int k) {
   if (MODE == BP_NORM) {
-    return __ldg(p + (size_t)clampi(j, 0, ny - 1) * nx + clampi(k, 0, nx - 1));
+    return to_f(__ldg(p + (size_t)clampi(j, 0, ny - 1) * nx + clampi(k, 0, nx - 1))) * sc;
   } else {
     const bool in = (unsigned)j < (unsigned)ny && (unsigned)k < (unsigned)nx;
     if (MODE == BP_WEIGHTS) return in ? 1.f : 0.f;
-    return in ? __ldg(p + (size_t)j * nx + k) : 0.f;
+    return in ? to_f(__ldg(p + (size_t)j * nx + k)) * sc : 0.f;
   }
 }
 
 // Separable staging: blended row value at column k (BP_NORM: k is clamped).
-template <int MODE>
-__device__ __forceinline__ float sep_at(const float *p, int nx, int ny,
+template <int MODE, typename IT>
+__device__ __forceinline__ float sep_at(const IT *p, float sc, int nx, int ny,
                                         const SepW &s, int k) {
   if (MODE == BP_NORM) {
     const float c = s.w0 + s.w1;
     const int kc = clampi(k, 0, nx - 1);
-    const float p0 = s.w0 != 0.f ? __ldg(p + (size_t)s.y0 * nx + kc) : 0.f;
-    const float p1 = s.w1 != 0.f ? __ldg(p + (size_t)(s.y0 + 1) * nx + kc) : 0.f;
+    const float p0 = s.w0 != 0.f ? to_f(__ldg(p + (size_t)s.y0 * nx + kc)) * sc : 0.f;
+    const float p1 = s.w1 != 0.f ? to_f(__ldg(p + (size_t)(s.y0 + 1) * nx + kc)) * sc : 0.f;
     return (s.w0 * p0 + s.w1 * p1) / c;
   } else {
     if ((unsigned)k >= (unsigned)nx) return 0.f;
     if (MODE == BP_WEIGHTS) return s.w0 + s.w1;
-    const float p0 = s.w0 != 0.f ? __ldg(p + (size_t)s.y0 * nx + k) : 0.f;
-    const float p1 = s.w1 != 0.f ? __ldg(p + (size_t)(s.y0 + 1) * nx + k) : 0.f;
+    const float p0 = s.w0 != 0.f ? to_f(__ldg(p + (size_t)s.y0 * nx + k)) * sc : 0.f;
+    const float p1 = s.w1 != 0.f ? to_f(__ldg(p + (size_t)(s.y0 + 1) * nx + k)) * sc : 0.f;
     return s.w0 * p0 + s.w1 * p1;
   }
 }
 
 // Interpolation of one staged chunk of tilts into the thread's accumulators.
-template <int MODE, bool SEP>
-__device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], const void *tblv,
+// Adds val to a voxel accumulator; with KAHAN the running compensation c
+// carries the low-order bits lost by each addition (compensated summation).
+template <bool KAHAN>
+__device__ __forceinline__ void acc_add(float &acc, float &c, float val) {
+  if (KAHAN) {
+    const float y = val - c;
+    const float t = acc + y;
+    c = (t - acc) - y;
+    acc = t;
+  } else {
+    acc += val;
+  }
+}
+
+template <int MODE, bool SEP, bool KAHAN>
+__device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kNV],
+                                              const void *tblv,
                                               const TileTilt *tt, const TiltGeo *geo,
                                               int nc, int per, int fw, int pny,
                                               int lane, int wy, int wz) {
@@ -164,7 +188,7 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], const void *tbl
 #pragma unroll
       for (int k = 0; k < kNV; ++k) {
         const float2 t = T[(int)(U >> 32)];
-        acc[k] += fmaf(one_plus_frac(U), t.y, t.x);
+        acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac(U), t.y, t.x));
         U += (unsigned long long)A2;
       }
     } else {
@@ -182,7 +206,7 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], const void *tbl
           const float f = one_plus_frac(U);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
           const float val = fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
-          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) acc[k] += val;
+          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) acc_add<KAHAN>(acc[k], cmp[k], val);
           U += (unsigned long long)A2;
           V += (unsigned long long)B2;
         }
@@ -194,7 +218,7 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], const void *tbl
           const float2 t0 = e[0], t1 = e[fw];
           const float f = one_plus_frac(U);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          acc[k] += fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
+          acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0));
           U += (unsigned long long)A2;
           V += (unsigned long long)B2;
         }
@@ -226,9 +250,10 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs &a, const float (&acc)[
 
 // Back-projection with tables staged by the threads from global memory (any
 // image width; also the voxel-weight pass, which has no image).
-template <int MODE, bool SEP>
+template <int MODE, bool SEP, typename IT>
 __global__ void __launch_bounds__(kThreads)
     bp_kernel(const BpArgs a) {
+  constexpr bool KAHAN = !std::is_same<IT, float>::value;
   extern __shared__ float4 tbl_raw[];
   float2 *tbl2 = reinterpret_cast<float2 *>(tbl_raw);
   __shared__ TileTilt tt[kMaxChunk];
@@ -243,9 +268,9 @@ __global__ void __launch_bounds__(kThreads)
   const int fw = a.fw, fh = SEP ? kTY : a.fh;
   const int pnx = a.img.nx, pny = a.img.ny;
 
-  float acc[kNV];
+  float acc[kNV], cmp[kNV];
 #pragma unroll
-  for (int k = 0; k < kNV; ++k) acc[k] = 0.f;
+  for (int k = 0; k < kNV; ++k) acc[k] = cmp[k] = 0.f;
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
@@ -261,30 +286,32 @@ __global__ void __launch_bounds__(kThreads)
       const int i = e / per, rq = e - i * per;
       const int r = rq / fw, q = rq - r * fw;
       if (r >= tt[i].nr || q >= tt[i].nq) continue;
-      const float *p = a.img.p ? a.img.p + (size_t)(a.t0 + c0 + i) * a.img.tstride
-                               : nullptr;
+      const int tilt = a.t0 + c0 + i;
+      const IT *p = a.img.p ? reinterpret_cast<const IT *>(a.img.p) + (size_t)tilt * a.img.tstride
+                            : nullptr;
+      const float sc = a.img.scale ? a.img.scale[tilt] : 1.f;
       const int x0 = tt[i].kmin + q;
       if (SEP) {
         const SepW s = sw[i][r];
         const bool valid = (MODE != BP_NORM) ||
                            ((s.w0 + s.w1) != 0.f && x0 >= -1 && x0 <= pnx - 1);
-        const float b = valid ? sep_at<MODE>(p, pnx, pny, s, x0) : 0.f;
-        const float n = valid ? sep_at<MODE>(p, pnx, pny, s, x0 + 1) : 0.f;
+        const float b = valid ? sep_at<MODE>(p, sc, pnx, pny, s, x0) : 0.f;
+        const float n = valid ? sep_at<MODE>(p, sc, pnx, pny, s, x0 + 1) : 0.f;
         const float sl = n - b;
         tbl2[e] = make_float2(b - sl, sl);
       } else {
         const int j = tt[i].jmin + r;
         const bool valid = (MODE != BP_NORM) ||
                            (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny);
-        const float b = valid ? img_at<MODE>(p, pnx, pny, j, x0) : 0.f;
-        const float n = valid ? img_at<MODE>(p, pnx, pny, j, x0 + 1) : 0.f;
+        const float b = valid ? img_at<MODE>(p, sc, pnx, pny, j, x0) : 0.f;
+        const float n = valid ? img_at<MODE>(p, sc, pnx, pny, j, x0 + 1) : 0.f;
         const float sl = n - b;
         tbl2[e] = make_float2(b - sl, sl);
       }
     }
     __syncthreads();
-    bp_accumulate<MODE, SEP>(acc, tbl_raw, tt, a.geo + a.t0 + c0, nc, per, fw, pny, lane,
-                             wy, wz);
+    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tbl_raw, tt, a.geo + a.t0 + c0, nc, per, fw,
+                                    pny, lane, wy, wz);
     __syncthreads();
   }
   bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
@@ -294,13 +321,15 @@ __global__ void __launch_bounds__(kThreads)
 //
 // One elected thread issues, per tilt, a 3-D bulk tensor copy (TMA,
 // cp.async.bulk.tensor, no multicast) of the tile's raw detector window --
-// columns [kmin & ~3, +BW), rows [ys, +BH) of image `tilt` -- into a raw
+// columns [kmin rounded down to 16 bytes, +BW), rows [ys, +BH) of image
+// `tilt` -- into a raw
 // shared buffer; the copies of the next chunk land while the CTA interpolates
 // the current one (two raw buffers, one mbarrier each).  TMA fills the parts
 // of a box outside the image with zeros.  The threads then turn the raw window
 // into interpolation-table entries with shared-memory reads only.  The global
-// tensor needs 16-byte row strides, so this path serves images whose width is
-// a multiple of 4; the others stage through bp_kernel.
+// tensor needs 16-byte row strides, so this path serves images whose rows are
+// a multiple of 16 bytes (width % 4 for float, % 8 for 16-bit elements); the
+// others stage through bp_kernel.
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -344,9 +373,10 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-template <int MODE, bool SEP>
+template <int MODE, bool SEP, typename IT>
 __global__ void __launch_bounds__(kThreads)
     bp_tma_kernel(const BpArgs a, const __grid_constant__ CUtensorMap tmap) {
+  constexpr bool KAHAN = !std::is_same<IT, float>::value;
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) unsigned long long mbar[2];
 
@@ -358,13 +388,14 @@ __global__ void __launch_bounds__(kThreads)
   const int zc = zl + a.v.zoff;
   const int fw = a.fw, fh = SEP ? kTY : a.fh;
   const int pnx = a.img.nx, pny = a.img.ny;
-  const int bw = a.tma_bw, bh = a.tma_bh, rs = a.tma_raw_stride;  // floats
+  const int bw = a.tma_bw, bh = a.tma_bh, rs = a.tma_raw_stride;  // elements
   const int nt = a.nt, chunk = a.chunk, per = fh * fw;
 
   TileTilt *tt = reinterpret_cast<TileTilt *>(dsm);
   SepW(*sw)[kTY] = reinterpret_cast<SepW(*)[kTY]>(dsm + (size_t)nt * sizeof(TileTilt));
-  float *raw0 = reinterpret_cast<float *>(dsm + a.tma_raw_offset);
-  float *tblf = raw0 + 2 * (size_t)chunk * rs;  // table entries (float2)
+  IT *raw0 = reinterpret_cast<IT *>(dsm + a.tma_raw_offset);
+  float *tblf = reinterpret_cast<float *>(raw0 + 2 * (size_t)chunk * rs);  // float2 entries
+  constexpr int kXAlign = 16 / (int)sizeof(IT);  // TMA x coordinates: 16-byte multiples
   float2 *tbl2 = reinterpret_cast<float2 *>(tblf);
 
   for (int i = tid; i < nt; i += kThreads) {
@@ -387,20 +418,20 @@ __global__ void __launch_bounds__(kThreads)
   auto issue = [&](int c, int buf) {
     const int c0 = c * chunk, nc = min(chunk, nt - c0);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&mbar[buf], (unsigned)(nc * bw * bh * 4));
-    float *dst = raw0 + (size_t)buf * chunk * rs;
+    mbar_expect_tx(&mbar[buf], (unsigned)(nc * bw * bh * (int)sizeof(IT)));
+    IT *dst = raw0 + (size_t)buf * chunk * rs;
     for (int i = 0; i < nc; ++i)
-      tma_load_3d(dst + (size_t)i * rs, &tmap, tt[c0 + i].kmin & ~3, tt[c0 + i].jmin,
-                  a.t0 + c0 + i, &mbar[buf]);
+      tma_load_3d(dst + (size_t)i * rs, &tmap, tt[c0 + i].kmin & ~(kXAlign - 1),
+                  tt[c0 + i].jmin, a.t0 + c0 + i, &mbar[buf]);
   };
   if (tid == 0) {
     issue(0, 0);
     if (nchunks > 1) issue(1, 1);
   }
 
-  float acc[kNV];
+  float acc[kNV], cmp[kNV];
 #pragma unroll
-  for (int k = 0; k < kNV; ++k) acc[k] = 0.f;
+  for (int k = 0; k < kNV; ++k) acc[k] = cmp[k] = 0.f;
 
   for (int c = 0; c < nchunks; ++c) {
     const int buf = c & 1, c0 = c * chunk, nc = min(chunk, nt - c0);
@@ -420,29 +451,32 @@ __global__ void __launch_bounds__(kThreads)
         mbar_wait_bounded(&mbar[buf ^ 1], (unsigned)(((c + 1) >> 1) & 1), 1ll << 28, nullptr);
       return;
     }
-    const float *R0 = raw0 + (size_t)buf * chunk * rs;
+    const IT *R0 = raw0 + (size_t)buf * chunk * rs;
     for (int e = tid; e < nc * per; e += kThreads) {
       const int i = e / per, rq = e - i * per;
       const int r = rq / fw, q = rq - r * fw;
       const TileTilt &t = tt[c0 + i];
       if (r >= t.nr || q >= t.nq) continue;
-      const float *R = R0 + (size_t)i * rs;
-      const int xs = t.kmin & ~3, ys = t.jmin;
+      const IT *R = R0 + (size_t)i * rs;
+      const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
+      const int xs = t.kmin & ~(kXAlign - 1), ys = t.jmin;
       const int x0 = t.kmin + q;
       if (SEP) {
         const SepW s = sw[c0 + i][r];
-        const float *r0 = R + (s.y0 - ys) * bw - xs, *r1 = r0 + bw;
+        const IT *r0 = R + (s.y0 - ys) * bw - xs, *r1 = r0 + bw;
         float b = 0.f, n = 0.f;
         if (MODE == BP_NORM) {
           if ((s.w0 + s.w1) != 0.f && x0 >= -1 && x0 <= pnx - 1) {
             const int kb = clampi(x0, 0, pnx - 1), kn = clampi(x0 + 1, 0, pnx - 1);
             const float c = s.w0 + s.w1;
-            b = (s.w0 * (s.w0 != 0.f ? r0[kb] : 0.f) + s.w1 * (s.w1 != 0.f ? r1[kb] : 0.f)) / c;
-            n = (s.w0 * (s.w0 != 0.f ? r0[kn] : 0.f) + s.w1 * (s.w1 != 0.f ? r1[kn] : 0.f)) / c;
+            const float w0 = s.w0 * sc, w1 = s.w1 * sc;
+            b = (w0 * (s.w0 != 0.f ? to_f(r0[kb]) : 0.f) + w1 * (s.w1 != 0.f ? to_f(r1[kb]) : 0.f)) / c;
+            n = (w0 * (s.w0 != 0.f ? to_f(r0[kn]) : 0.f) + w1 * (s.w1 != 0.f ? to_f(r1[kn]) : 0.f)) / c;
           }
         } else {
-          b = s.w0 * r0[x0] + s.w1 * r1[x0];
-          n = s.w0 * r0[x0 + 1] + s.w1 * r1[x0 + 1];
+          const float w0 = s.w0 * sc, w1 = s.w1 * sc;
+          b = w0 * to_f(r0[x0]) + w1 * to_f(r1[x0]);
+          n = w0 * to_f(r0[x0 + 1]) + w1 * to_f(r1[x0 + 1]);
         }
         const float sl = n - b;
         tbl2[e] = make_float2(b - sl, sl);
@@ -451,14 +485,14 @@ __global__ void __launch_bounds__(kThreads)
         float b = 0.f, n = 0.f;
         if (MODE == BP_NORM) {
           if (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny) {
-            const float *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
-            b = row[clampi(x0, 0, pnx - 1)];
-            n = row[clampi(x0 + 1, 0, pnx - 1)];
+            const IT *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
+            b = to_f(row[clampi(x0, 0, pnx - 1)]) * sc;
+            n = to_f(row[clampi(x0 + 1, 0, pnx - 1)]) * sc;
           }
         } else {
-          const float *row = R + r * bw - xs;
-          b = row[x0];
-          n = row[x0 + 1];
+          const IT *row = R + r * bw - xs;
+          b = to_f(row[x0]) * sc;
+          n = to_f(row[x0 + 1]) * sc;
         }
         const float sl = n - b;
         tbl2[e] = make_float2(b - sl, sl);
@@ -466,8 +500,8 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     if (tid == 0 && c + 2 < nchunks) issue(c + 2, buf);
-    bp_accumulate<MODE, SEP>(acc, tblf, tt + c0, a.geo + a.t0 + c0, nc, per, fw, pny, lane,
-                             wy, wz);
+    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tblf, tt + c0, a.geo + a.t0 + c0, nc, per, fw,
+                                    pny, lane, wy, wz);
     __syncthreads();
   }
   bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
@@ -673,6 +707,88 @@ __global__ void resid_kernel(const float *__restrict__ p, float *val,
   }
 }
 
+// ------------------------------------------------------ 16-bit storage
+//
+// Measured projections and SIRT residuals may be stored as FP16 or BF16 to
+// halve the bytes staged per tilt.  A stored element e of tilt t stands for
+// e * scale[t]; the scales are powers of two, so scaling is exact and the
+// only rounding is the 16-bit conversion itself.
+
+template <typename T>
+__device__ __forceinline__ T from_f(float x);
+template <>
+__device__ __forceinline__ float from_f<float>(float x) { return x; }
+template <>
+__device__ __forceinline__ __half from_f<__half>(float x) { return __float2half_rn(x); }
+template <>
+__device__ __forceinline__ __nv_bfloat16 from_f<__nv_bfloat16>(float x) {
+  return __float2bfloat16_rn(x);
+}
+
+// 2^e as a float for |e| < 127.
+__device__ __forceinline__ float pow2f(int e) { return __int_as_float((127 + e) << 23); }
+
+// Per-tilt maximum of |p| as float bits (non-negative floats order like their
+// bit patterns).  grid.y = tilt.
+__global__ void absmax_kernel(const float *__restrict__ p, size_t plane,
+                              unsigned *__restrict__ maxbits) {
+  const float *pt = p + plane * blockIdx.y;
+  float m = 0.f;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float v = fabsf(pt[i]);
+    m = v > m ? v : m;  // NaN never replaces m
+  }
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(maxbits + blockIdx.y, __float_as_uint(m));
+}
+
+// Exponent e of the power-of-two scale of a tilt whose largest magnitude has
+// float bits mb: FP16 places the maximum in (2^13, 2^14], a factor of four
+// below the format's largest finite value, so residuals up to four times the
+// measured range stay finite; BF16 has float's range and keeps scale 1.
+template <typename T>
+__device__ __forceinline__ int scale_exp(unsigned mb) {
+  if (!std::is_same<T, __half>::value || mb == 0u || mb >= 0x7f800000u) return 0;
+  const int E = (int)(mb >> 23) - 127;  // m = 1.f * 2^E, f the fraction bits
+  const int ceil_log2 = (mb & 0x7fffffu) ? E + 1 : E;
+  return max(-126, min(126, ceil_log2 - 14));
+}
+
+template <typename T>
+__global__ void quantize_kernel(const float *__restrict__ p, size_t plane,
+                                const unsigned *__restrict__ maxbits, T *__restrict__ out,
+                                float *__restrict__ scale) {
+  const int t = blockIdx.y;
+  const int e = scale_exp<T>(maxbits[t]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) scale[t] = pow2f(e);
+  const float inv = pow2f(-e);
+  const float *pt = p + plane * t;
+  T *ot = out + plane * t;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane;
+       i += (size_t)gridDim.x * blockDim.x)
+    ot[i] = from_f<T>(pt[i] * inv);
+}
+
+// SIRT residual from 16-bit measured projections: r = p*ps[t] - val/wt (val
+// where wt == 0), stored as RT in units of rs[t] (rs == nullptr: 1).  With
+// RT = float, r may alias val.  grid.y = tilt.
+template <typename PT, typename RT>
+__global__ void resid_lp_kernel(const PT *__restrict__ p, const float *__restrict__ ps,
+                                const float *val, const float *__restrict__ wt, size_t plane,
+                                RT *r, const float *__restrict__ rs) {
+  const size_t off = plane * blockIdx.y;
+  const float sp = ps ? ps[blockIdx.y] : 1.f;
+  const float inv = rs ? 1.f / rs[blockIdx.y] : 1.f;  // exact: rs is a power of two
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < plane;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float v = val[off + i];
+    const float w = wt[off + i];
+    if (w != 0.f) v /= w;
+    r[off + i] = from_f<RT>((to_f(p[off + i]) * sp - v) * inv);
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 
 static dim3 tile_grid(const VolView &v) {
@@ -680,15 +796,15 @@ static dim3 tile_grid(const VolView &v) {
               (v.nz + kTZ - 1) / kTZ);
 }
 
-template <int MODE, bool SEP>
+template <int MODE, bool SEP, typename IT>
 static cudaError_t launch_bp_t(const BpArgs &a, cudaStream_t s) {
   const int fh = SEP ? kTY : a.fh;
   const size_t smem = (size_t)a.chunk * fh * a.fw * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(
-      bp_kernel<MODE, SEP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      bp_kernel<MODE, SEP, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
       (int)smem);
   if (e != cudaSuccess) return e;
-  bp_kernel<MODE, SEP><<<tile_grid(a.v), kThreads, smem, s>>>(a);
+  bp_kernel<MODE, SEP, IT><<<tile_grid(a.v), kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -715,19 +831,29 @@ constexpr size_t kSmemTma = 56 * 1024;
 
 // TMA-staged launch; returns false (nothing launched) when the image or the
 // window does not fit the TMA path.
-template <int MODE, bool SEP>
+template <typename IT>
+constexpr CUtensorMapDataType tma_type() {
+  return std::is_same<IT, float>::value   ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+         : std::is_same<IT, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                           : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+}
+
+template <int MODE, bool SEP, typename IT>
 static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err) {
   const ImgView &im = a0.img;
-  if (!im.p || !a0.err || im.nx % 4 != 0 || (reinterpret_cast<uintptr_t>(im.p) & 15) != 0)
+  constexpr int es = (int)sizeof(IT);
+  constexpr int xal = 16 / es;  // TMA x coordinates and box widths: 16-byte multiples
+  if (!im.p || !a0.err || (im.nx * es) % 16 != 0 ||
+      (reinterpret_cast<uintptr_t>(im.p) & 15) != 0)
     return false;
   const int fh = SEP ? kTY : a0.fh;
-  const int bw = (a0.fw + 4 + 3) & ~3;
+  const int bw = (a0.fw + xal + xal - 1) / xal * xal;
   const int bh = SEP ? kTY + 3 : fh + 1;
   if (bw > 256 || bh > 256) return false;
-  const int rs = (bw * bh + 31) & ~31;  // floats; 128-byte aligned raw slots
+  const int rs = ((bw * bh * es + 127) & ~127) / es;  // elements; 128-byte aligned slots
   const size_t fixed =
       ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
-  const size_t per_tilt = 2 * (size_t)rs * 4 + (size_t)fh * a0.fw * sizeof(float2);
+  const size_t per_tilt = 2 * (size_t)rs * es + (size_t)fh * a0.fw * sizeof(float2);
   if (fixed + per_tilt > kSmemTma + 64 * 1024) return false;
   int chunk = (int)std::max<size_t>(1, (kSmemTma > fixed ? kSmemTma - fixed : 0) / per_tilt);
   chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
@@ -737,11 +863,11 @@ static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err
   CUtensorMap map;
   const cuuint64_t dims[3] = {(cuuint64_t)im.nx, (cuuint64_t)im.ny,
                               (cuuint64_t)(a0.t0 + a0.nt)};
-  const cuuint64_t strides[2] = {(cuuint64_t)im.nx * 4, (cuuint64_t)im.tstride * 4};
+  const cuuint64_t strides[2] = {(cuuint64_t)im.nx * es, (cuuint64_t)im.tstride * es};
   const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(im.p), dims, strides,
-          box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+  if (enc(&map, tma_type<IT>(), 3, const_cast<float *>(im.p), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   BpArgs a = a0;
@@ -750,34 +876,42 @@ static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err
   a.tma_bh = bh;
   a.tma_raw_stride = rs;
   a.tma_raw_offset = (int)fixed;
-  cudaError_t e = cudaFuncSetAttribute(bp_tma_kernel<MODE, SEP>,
+  cudaError_t e = cudaFuncSetAttribute(bp_tma_kernel<MODE, SEP, IT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
-    bp_tma_kernel<MODE, SEP><<<tile_grid(a.v), kThreads, smem, s>>>(a, map);
+    bp_tma_kernel<MODE, SEP, IT><<<tile_grid(a.v), kThreads, smem, s>>>(a, map);
     e = cudaGetLastError();
   }
   *err = e;
   return true;
 }
 
-template <int MODE, bool SEP>
+template <int MODE, bool SEP, typename IT>
 static cudaError_t launch_bp_any(const BpArgs &a, cudaStream_t s) {
   if (MODE != BP_WEIGHTS) {
     cudaError_t e;
-    if (try_launch_bp_tma<MODE, SEP>(a, s, &e)) return e;
+    if (try_launch_bp_tma<MODE, SEP, IT>(a, s, &e)) return e;
   }
-  return launch_bp_t<MODE, SEP>(a, s);
+  return launch_bp_t<MODE, SEP, IT>(a, s);
+}
+
+template <typename IT>
+static cudaError_t launch_bp_it(int mode, bool sep, const BpArgs &a, cudaStream_t s) {
+  if (sep) {
+    if (mode == BP_NORM) return launch_bp_any<BP_NORM, true, IT>(a, s);
+    return launch_bp_any<BP_SIRT, true, IT>(a, s);
+  }
+  if (mode == BP_NORM) return launch_bp_any<BP_NORM, false, IT>(a, s);
+  return launch_bp_any<BP_SIRT, false, IT>(a, s);
 }
 
 cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s) {
-  if (sep) {
-    if (mode == BP_NORM) return launch_bp_any<BP_NORM, true>(a, s);
-    if (mode == BP_SIRT) return launch_bp_any<BP_SIRT, true>(a, s);
-    return launch_bp_any<BP_WEIGHTS, true>(a, s);
-  }
-  if (mode == BP_NORM) return launch_bp_any<BP_NORM, false>(a, s);
-  if (mode == BP_SIRT) return launch_bp_any<BP_SIRT, false>(a, s);
-  return launch_bp_any<BP_WEIGHTS, false>(a, s);
+  if (mode == BP_WEIGHTS)
+    return sep ? launch_bp_any<BP_WEIGHTS, true, float>(a, s)
+               : launch_bp_any<BP_WEIGHTS, false, float>(a, s);
+  if (a.img.dtype == IMG_F16) return launch_bp_it<__half>(mode, sep, a, s);
+  if (a.img.dtype == IMG_BF16) return launch_bp_it<__nv_bfloat16>(mode, sep, a, s);
+  return launch_bp_it<float>(mode, sep, a, s);
 }
 
 static dim3 fp_grid(const VolView &v) {
@@ -807,6 +941,53 @@ cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
                          int nsm, cudaStream_t s) {
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
   resid_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(p, val, wt, n);
+  return cudaGetLastError();
+}
+
+static unsigned plane_blocks(size_t plane, int nt, int nsm) {
+  // About 8 resident 256-thread blocks per SM in total across the tilts.
+  const size_t want = ((size_t)nsm * 8 + nt - 1) / nt;
+  const size_t need = (plane + 255) / 256;
+  return (unsigned)std::max<size_t>(1, std::min(want, need));
+}
+
+cudaError_t launch_quantize(const float *p, size_t plane, int nt, int dtype, void *out,
+                            float *scale, unsigned *maxbits, int nsm, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned) * nt, s);
+  if (e != cudaSuccess) return e;
+  const dim3 grid(plane_blocks(plane, nt, nsm), nt);
+  absmax_kernel<<<grid, 256, 0, s>>>(p, plane, maxbits);
+  if (dtype == IMG_F16)
+    quantize_kernel<__half><<<grid, 256, 0, s>>>(p, plane, maxbits, (__half *)out, scale);
+  else
+    quantize_kernel<__nv_bfloat16><<<grid, 256, 0, s>>>(p, plane, maxbits,
+                                                        (__nv_bfloat16 *)out, scale);
+  return cudaGetLastError();
+}
+
+template <typename PT>
+static void resid_lp_rt(const PT *p, const float *ps, const float *val, const float *wt,
+                        size_t plane, int nt, int rdtype, void *r, const float *rs,
+                        int nsm, cudaStream_t s) {
+  const dim3 grid(plane_blocks(plane, nt, nsm), nt);
+  if (rdtype == IMG_F16)
+    resid_lp_kernel<PT, __half><<<grid, 256, 0, s>>>(p, ps, val, wt, plane, (__half *)r, rs);
+  else if (rdtype == IMG_BF16)
+    resid_lp_kernel<PT, __nv_bfloat16><<<grid, 256, 0, s>>>(p, ps, val, wt, plane,
+                                                            (__nv_bfloat16 *)r, rs);
+  else
+    resid_lp_kernel<PT, float><<<grid, 256, 0, s>>>(p, ps, val, wt, plane, (float *)r, rs);
+}
+
+cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const float *val,
+                            const float *wt, size_t plane, int nt, int rdtype, void *r,
+                            const float *rs, int nsm, cudaStream_t s) {
+  if (pdtype == IMG_F16)
+    resid_lp_rt((const __half *)p, ps, val, wt, plane, nt, rdtype, r, rs, nsm, s);
+  else if (pdtype == IMG_BF16)
+    resid_lp_rt((const __nv_bfloat16 *)p, ps, val, wt, plane, nt, rdtype, r, rs, nsm, s);
+  else
+    resid_lp_rt((const float *)p, ps, val, wt, plane, nt, rdtype, r, rs, nsm, s);
   return cudaGetLastError();
 }
 

@@ -193,6 +193,8 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   bp.img.nx = nx;
   bp.img.ny = ny;
   bp.img.tstride = (long long)nx * ny;
+  bp.img.dtype = IMG_F32;
+  bp.img.scale = nullptr;
   bp.geo = geo;
   bp.t0 = 0;
   bp.nt = nt;

@@ -153,3 +153,34 @@ def add_noise(proj, cfg: Config, seed_offset: int = 7):
     rng = np.random.default_rng(cfg.seed + seed_offset)
     sigma = cfg.noise * float(p.std())
     return (p + rng.normal(0.0, sigma, p.shape)).astype(np.float32)
+
+
+def project_series(engine, cfg: Config, layout: int = 0, noise: str = "gaussian",
+                   mean_counts: float = 20.0):
+    """Tilt series of ``cfg``'s phantom on the device, projected with the
+    engine's forward model (val/wt where wt != 0) under the problem already
+    set on ``engine``; returns a contiguous float32 CUDA tensor [nt][ny][nx].
+
+    noise: ``"gaussian"`` adds sigma = cfg.noise * std; ``"poisson"`` maps the
+    projections linearly onto [0, 2 * mean_counts] and draws counting noise
+    (electrons per pixel); ``"none"`` leaves them clean.  Seeded from
+    cfg.seed."""
+    import torch
+    nx, ny, nt = cfg.nx, cfg.ny, cfg.ntilt
+    ph = phantom(cfg, layout, device="cuda")
+    val = torch.zeros((nt, ny, nx), device="cuda")
+    wt = torch.zeros_like(val)
+    engine.forward_project(ph, val, wt)
+    proj = torch.where(wt != 0, val / torch.where(wt != 0, wt, 1), 0)
+    del ph, val, wt
+    g = torch.Generator(device="cuda").manual_seed(cfg.seed + 7)
+    if noise == "gaussian":
+        proj += cfg.noise * proj.std() * torch.randn(proj.shape, device="cuda", generator=g)
+    elif noise == "poisson":
+        lo, hi = proj.min(), proj.max()
+        proj = (proj - lo) * (2.0 * mean_counts / torch.clamp(hi - lo, min=1e-30))
+        proj = torch.poisson(proj, generator=g)
+    elif noise != "none":
+        raise ValueError(noise)
+    torch.cuda.synchronize()
+    return proj.contiguous()

@@ -37,6 +37,15 @@ LAYOUT_Y, LAYOUT_Z = 0, 1
 METHOD_BPT, METHOD_WBP, METHOD_SIRT, METHOD_SART = 0, 1, 2, 3
 METHODS = {"BPT": METHOD_BPT, "WBP": METHOD_WBP, "SIRT": METHOD_SIRT,
            "SART": METHOD_SART}
+DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
+DTYPES = {"f32": DTYPE_F32, "f16": DTYPE_F16, "bf16": DTYPE_BF16}
+
+
+def _dtype_code(t) -> int:
+    """tr_dtype of a torch tensor's element type."""
+    import torch
+    return {torch.float32: DTYPE_F32, torch.float16: DTYPE_F16,
+            torch.bfloat16: DTYPE_BF16}[t.dtype]
 
 _lib = None
 
@@ -85,6 +94,9 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_sart.argtypes = [vp, vp, vp, i, f, vp]
     lib.tr_wbp.argtypes = [vp, vp, vp, vp]
     lib.tr_reconstruct_host.argtypes = [vp, i, vp, vp, i, f]
+    lib.tr_quantize.argtypes = [vp, vp, i, vp, vp, vp]
+    lib.tr_backproject_lp.argtypes = [vp, vp, i, vp, vp, i, i, vp]
+    lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
     lib.tr_synchronize.argtypes = [vp]
     for name in ("tr_create", "tr_destroy", "tr_set_problem", "tr_update_geometry",
                  "tr_filter_rweight",
@@ -222,6 +234,29 @@ class Engine:
         self._check(self.lib.tr_reconstruct_host(self.h, m, proj.ctypes.data,
                                                  vol.ctypes.data, iters, gamma),
                     "tr_reconstruct_host")
+
+    def quantize(self, proj, dtype):
+        """FP32 stack -> (16-bit stack, per-tilt power-of-two scales), new
+        CUDA tensors; dtype is torch.float16 or torch.bfloat16."""
+        import torch
+        out = torch.empty(proj.shape, dtype=dtype, device=proj.device)
+        scale = torch.empty(proj.shape[0], dtype=torch.float32, device=proj.device)
+        self._check(self.lib.tr_quantize(self.h, _ptr(proj), _dtype_code(out), _ptr(out),
+                                         _ptr(scale), _stream(self.device)), "tr_quantize")
+        return out, scale
+
+    def backproject_lp(self, proj, scale, vol, z0=0, nz=None):
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_backproject_lp(self.h, _ptr(proj), _dtype_code(proj),
+                                               _ptr(scale), _ptr(vol), z0, nz,
+                                               _stream(self.device)), "tr_backproject_lp")
+
+    def sirt_lp(self, proj, scale, vol, iters, gamma, resid_dtype="bf16"):
+        """SIRT from a 16-bit stack (see :meth:`quantize`); resid_dtype is
+        'f32', 'f16' or 'bf16'."""
+        self._check(self.lib.tr_sirt_lp(self.h, _ptr(proj), _dtype_code(proj), _ptr(scale),
+                                        DTYPES[resid_dtype], _ptr(vol), iters, gamma,
+                                        _stream(self.device)), "tr_sirt_lp")
 
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")

@@ -121,17 +121,7 @@ def make_series(eng, torch, cfg, coeff):
     projected with the engine's forward model (val/wt), plus Gaussian noise
     of 0.3 x std.  Input generation only; it is outside the timed region."""
     from autom2_b200 import synth
-    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
-    ph = synth.phantom(cfg, device="cuda")
-    val = torch.zeros((nt, ny, nx), device="cuda")
-    wt = torch.zeros_like(val)
-    eng.forward_project(ph, val, wt)
-    proj = torch.where(wt != 0, val / torch.where(wt != 0, wt, 1), 0)
-    g = torch.Generator(device="cuda").manual_seed(cfg.seed + 7)
-    proj += cfg.noise * proj.std() * torch.randn(proj.shape, device="cuda", generator=g)
-    del ph, val, wt
-    torch.cuda.synchronize()
-    return proj.contiguous()
+    return synth.project_series(eng, cfg, 0, "gaussian")
 
 
 def cpu_baseline(cfg, coeff, proj_np, target_s: float = 12.0):

@@ -63,6 +63,13 @@ typedef enum {
   TR_METHOD_SART = 3   /* SART,n,gamma                       */
 } tr_method;
 
+/* Element types of 16-bit storage (projections, SIRT residuals). */
+typedef enum {
+  TR_DTYPE_F32 = 0,
+  TR_DTYPE_F16 = 1,  /* IEEE binary16 */
+  TR_DTYPE_BF16 = 2  /* bfloat16 */
+} tr_dtype;
+
 /* Library version: major*10000 + minor*100 + patch. */
 int tr_version(void);
 const char *tr_status_string(int status);
@@ -141,6 +148,32 @@ tr_status tr_wbp(tr_ctx *ctx, float *proj_dev, float *vol_dev, void *stream);
  * across calls of the same size. */
 tr_status tr_reconstruct_host(tr_ctx *ctx, int method, const float *proj_host,
                               float *vol_host, int iters, float gamma);
+
+/* Mixed precision.  No counterpart in the reference (whose projections and
+ * residuals are float throughout).  A 16-bit stack holds element e of tilt t
+ * for the value e * scale[t]; the per-tilt scales are powers of two.
+ *
+ * tr_quantize: FP32 stack proj_dev -> out_dev (ntilt*ny*nx elements of
+ * `dtype`, TR_DTYPE_F16 or TR_DTYPE_BF16) and scale_dev[ntilt].  FP16 scales
+ * put each tilt's largest magnitude in (2^13, 2^14], a factor of four under
+ * the format's largest finite value; BF16 keeps scale 1. */
+tr_status tr_quantize(tr_ctx *ctx, const float *proj_dev, int dtype,
+                      void *out_dev, float *scale_dev, void *stream);
+
+/* Back-projection (as tr_backproject) from a 16-bit stack; the FP32 sums
+ * over tilts are compensated (Kahan) per voxel. */
+tr_status tr_backproject_lp(tr_ctx *ctx, const void *proj_dev, int dtype,
+                            const float *scale_dev, float *vol_dev, int z0,
+                            int nz, void *stream);
+
+/* SIRT (as tr_sirt) from a 16-bit stack (proj_dtype, scales from
+ * tr_quantize) with the residual stored as resid_dtype (TR_DTYPE_F32, F16 --
+ * in the projections' per-tilt scale -- or BF16).  The reprojection,
+ * weights and volume stay FP32; the residual back-projection sums are
+ * compensated per voxel when the residual is 16-bit. */
+tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
+                     const float *scale_dev, int resid_dtype, float *vol_dev,
+                     int iters, float gamma, void *stream);
 
 /* SIRT that allocates no device memory and needs no context.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -79,10 +79,37 @@ def test_tiltrec_vs_tiltrec_mpi(case, method, geometry):
     # ceil(|tan(pitch)| * thickness) (main-mpi.cpp:728-740: the first branch
     # resets only add_left), so it reads that many rows past the end of the
     # stack (unread, uninitialised) and reconstructs them into the top
-    # sections.  Those sections are excluded; the rest must match.
+    # sections.  The rows they reach are excluded from the comparison with
+    # the reference (two for the one-pass methods; SART's per-tilt updates
+    # carry them two rows further: its row 36 still differs from the
+    # restatement by 1e-5, row 35 by 5e-7) and compared with the oracle
+    # restatement instead, which the whole volume must match.
     pitch = float(geometry.split(",")[1])
-    cut = slice(0, proj.shape[1] - 2) if pitch else None
+    cut = slice(0, proj.shape[1] - (4 if method.startswith("SART") else 2)) if pitch else None
     compare(a, b, sections=cut)
+    if pitch:
+        _, _, got = read_mrc(a)
+        assert O.rel_l2(got, restated(0, proj, ang, geometry, method)) < TOL
+
+
+def restated(layout, proj, ang, geometry, method):
+    """The oracle restatement's reconstruction for a CLI geometry/method."""
+    R = O.Restatement()
+    nt, ny, nx = proj.shape
+    off, pitch, zs, th = (float(v) for v in geometry.split(","))
+    th = int(th)
+    c8 = R.coeffs(ang, off, pitch, zs)
+    org = T.default_origin(layout, nx, ny, th)
+    g = R.geom(nx, ny, nt, th, layout, 0, org)
+    vshape = (ny, th, nx) if layout == 0 else (th, ny, nx)
+    zero = np.zeros(vshape, np.float32)
+    parts = method.split(",")
+    if parts[0] == "BPT":
+        return R.backproject(g, c8, proj, zero)
+    if parts[0] == "WBP":
+        return R.backproject(g, c8, R.filter_rweight(proj), zero)
+    f = R.sirt if parts[0] == "SIRT" else R.sart
+    return f(g, c8, proj, zero, int(parts[1]), float(parts[2]))
 
 
 def test_initial_volume(case):
