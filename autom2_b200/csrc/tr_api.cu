@@ -365,6 +365,9 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   if (ent_bp > kSmemMax || ent_fp > kSmemMax)
     return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds shared memory",
                 ffw, ffh);
+  if (std::max(std::max(fw, fh), std::max(ffw, ffh)) > kMaxWindow)
+    return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds %d",
+                std::max(fw, ffw), std::max(fh, ffh), kMaxWindow);
   if (s) {
     TR_CUDA(c, cudaMemcpyAsync(c->geo_d, g.data(), sizeof(TiltGeo) * nt,
                                cudaMemcpyHostToDevice, s));

@@ -23,6 +23,10 @@ constexpr int kFX = 2 * kTX;                  // 64
 constexpr int kFNV = 16;                      // voxel pairs per thread along z
 constexpr int kFTZ = kZG * kFNV;              // 32
 
+// Largest tile window side (columns or rows): the kernels step window
+// coordinates in Q9.23 fixed point, whose integer part is below 512.
+constexpr int kMaxWindow = 511;
+
 // Per-tilt projection geometry.  a/b are the reference's linear coefficients
 // (detector x = a0 + a1 X + a2 Y + a3 Z + ox, y likewise with b, X/Y/Z the
 // voxel offsets from the origin).  A/B are the same slopes in Q32.32 fixed

@@ -157,6 +157,38 @@ __device__ __forceinline__ float sep_at(const IT *p, float sc, int nx, int ny,
   }
 }
 
+// Position (tilt i, row r, column q) of table entry e in a chunk's tables laid
+// out [tilt][fh rows][fw columns], for e = tid, tid + kThreads, ...: the
+// divisions happen once per chunk and each step adds the precomputed
+// decomposition of kThreads.
+struct EntryWalk {
+  int i, r, q, si, sr, sq;
+  __device__ __forceinline__ EntryWalk(int e0, int fh, int fw) {
+    const int per = fh * fw;
+    i = e0 / per;
+    const int rq = e0 - i * per;
+    r = rq / fw;
+    q = rq - r * fw;
+    si = kThreads / per;
+    const int rem = kThreads - si * per;
+    sr = rem / fw;
+    sq = rem - sr * fw;
+  }
+  __device__ __forceinline__ void next(int fh, int fw) {
+    q += sq;
+    r += sr;
+    i += si;
+    if (q >= fw) {
+      q -= fw;
+      ++r;
+    }
+    if (r >= fh) {
+      r -= fh;
+      ++i;
+    }
+  }
+};
+
 // Interpolation of one staged chunk of tilts into the thread's accumulators.
 // Adds val to a voxel accumulator; with KAHAN the running compensation c
 // carries the low-order bits lost by each addition (compensated summation).
@@ -172,6 +204,17 @@ __device__ __forceinline__ void acc_add(float &acc, float &c, float val) {
   }
 }
 
+// Window coordinates inside the z loop run in Q9.23 (32-bit): the integer
+// part is the window column/row (< 512), the 23 fraction bits are exactly the
+// float mantissa of 1 + dx.  Each thread's start is the exact Q32.32 value
+// truncated; the per-voxel step is rounded to 2^-23, so after the kNV - 1
+// steps of a thread the coordinate is within 8 * 2^-23 px of the exact one.
+__device__ __forceinline__ unsigned q23(unsigned long long U) { return (unsigned)(U >> 9); }
+__device__ __forceinline__ unsigned q23_step(long long A) { return (unsigned)((A + 256) >> 9); }
+__device__ __forceinline__ float one_plus_frac23(unsigned u) {
+  return __uint_as_float(0x3F800000u | (u & 0x7FFFFFu));
+}
+
 template <int MODE, bool SEP, bool KAHAN>
 __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kNV],
                                               const void *tblv,
@@ -181,46 +224,48 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
   for (int i = 0; i < nc; ++i) {
     const TiltGeo &g = geo[i];
     const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
-    unsigned long long U = (unsigned long long)(tt[i].U0 + lane * A0 + wy * A1 +
-                                                (long long)(wz * kNV) * A2);
+    unsigned u = q23((unsigned long long)(tt[i].U0 + lane * A0 + wy * A1 +
+                                          (long long)(wz * kNV) * A2));
+    const unsigned du = q23_step(A2);
     if (SEP) {
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)(i * kTY + wy) * fw;
 #pragma unroll
       for (int k = 0; k < kNV; ++k) {
-        const float2 t = T[(int)(U >> 32)];
-        acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac(U), t.y, t.x));
-        U += (unsigned long long)A2;
+        const float2 t = T[u >> 23];
+        acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac23(u), t.y, t.x));
+        u += du;
       }
     } else {
       const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
-      unsigned long long V = (unsigned long long)(tt[i].V0 + lane * B0 + wy * B1 +
-                                                  (long long)(wz * kNV) * B2);
+      unsigned v = q23((unsigned long long)(tt[i].V0 + lane * B0 + wy * B1 +
+                                            (long long)(wz * kNV) * B2));
+      const unsigned dv = q23_step(B2);
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)i * per;
       const int jmin = tt[i].jmin;
       if (MODE == BP_NORM && tt[i].check_rows) {
 #pragma unroll
         for (int k = 0; k < kNV; ++k) {
-          const int q = (int)(U >> 32), r = (int)(V >> 32);
+          const int q = (int)(u >> 23), r = (int)(v >> 23);
           const float2 *e = T + r * fw + q;
           const float2 t0 = e[0], t1 = e[fw];
-          const float f = one_plus_frac(U);
+          const float f = one_plus_frac23(u);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          const float val = fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0);
+          const float val = fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
           if ((unsigned)(jmin + r + 1) <= (unsigned)pny) acc_add<KAHAN>(acc[k], cmp[k], val);
-          U += (unsigned long long)A2;
-          V += (unsigned long long)B2;
+          u += du;
+          v += dv;
         }
       } else {
 #pragma unroll
         for (int k = 0; k < kNV; ++k) {
-          const int q = (int)(U >> 32), r = (int)(V >> 32);
+          const int q = (int)(u >> 23), r = (int)(v >> 23);
           const float2 *e = T + r * fw + q;
           const float2 t0 = e[0], t1 = e[fw];
-          const float f = one_plus_frac(U);
+          const float f = one_plus_frac23(u);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac(V) - 1.f, r1 - r0, r0));
-          U += (unsigned long long)A2;
-          V += (unsigned long long)B2;
+          acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0));
+          u += du;
+          v += dv;
         }
       }
     }
@@ -282,9 +327,9 @@ __global__ void __launch_bounds__(kThreads)
     // chunk's entries keeps many independent image loads in flight per
     // thread; entries outside a tilt's reachable window are skipped.
     const int per = fh * fw;
-    for (int e = tid; e < nc * per; e += kThreads) {
-      const int i = e / per, rq = e - i * per;
-      const int r = rq / fw, q = rq - r * fw;
+    EntryWalk w(tid, fh, fw);
+    for (int e = tid; e < nc * per; e += kThreads, w.next(fh, fw)) {
+      const int i = w.i, r = w.r, q = w.q;
       if (r >= tt[i].nr || q >= tt[i].nq) continue;
       const int tilt = a.t0 + c0 + i;
       const IT *p = a.img.p ? reinterpret_cast<const IT *>(a.img.p) + (size_t)tilt * a.img.tstride
@@ -452,9 +497,9 @@ __global__ void __launch_bounds__(kThreads)
       return;
     }
     const IT *R0 = raw0 + (size_t)buf * chunk * rs;
-    for (int e = tid; e < nc * per; e += kThreads) {
-      const int i = e / per, rq = e - i * per;
-      const int r = rq / fw, q = rq - r * fw;
+    EntryWalk w(tid, fh, fw);
+    for (int e = tid; e < nc * per; e += kThreads, w.next(fh, fw)) {
+      const int i = w.i, r = w.r, q = w.q;
       const TileTilt &t = tt[c0 + i];
       if (r >= t.nr || q >= t.nq) continue;
       const IT *R = R0 + (size_t)i * rs;

@@ -125,6 +125,8 @@ bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
   const size_t ent_bp = (size_t)out->fw * out->fh * sizeof(float2);
   const size_t ent_fp = (size_t)out->ffw * out->ffh * sizeof(float);
   if (ent_bp > kStaticSmemMax || ent_fp > kStaticSmemMax) return false;
+  if (std::max(std::max(out->fw, out->fh), std::max(out->ffw, out->ffh)) > kMaxWindow)
+    return false;
   out->chunk_bp =
       (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemBp / ent_bp));
   out->chunk_fp =

@@ -340,6 +340,26 @@ def run_ours(args):
            "h2d_bytes_per_step": int(proj_np.nbytes + vol_np.nbytes),
            "d2h_bytes_per_step": int(vol_np.nbytes), "ms_per_step": e2e_s * 1e3}
 
+    # The same step with 16-bit storage: FP16 projections (per-tilt
+    # power-of-two scales) and an FP16 residual, FP32 volume and sums.
+    q, qscale = eng.quantize(proj, torch.float16)
+    torch.cuda.synchronize()
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    lp_steps = max(1, min(args.steps, 2))
+    l0.record(stream)
+    for _ in range(lp_steps):
+        eng.update_geometry(coeff)
+        vol.zero_()
+        eng.sirt_lp(q, qscale, vol, cfg.iters, cfg.gamma, "f16")
+    l1.record(stream)
+    torch.cuda.synchronize()
+    lp_ms = l0.elapsed_time(l1) / lp_steps
+    variants = {"sirt_f16_storage": {
+        "ms_per_step": lp_ms, "value": ws * vpu_step / (lp_ms / 1e3), "unit": UNIT,
+        "storage": "projections and residual FP16 (per-tilt scale), volume FP32",
+        "bytes_saved_per_iter": int(2 * nt * ny * nx * 2)}}
+    del q, qscale
+
     line = None
     if rank == 0:
         cb = cpu_baseline(cfg, coeff, proj.cpu().numpy()) if ws == 1 else None
@@ -355,7 +375,7 @@ def run_ours(args):
                            "parallelism": f"replicas x{ws}"},
                 "roofline": roofline, "cpu_baseline": cb, "e2e": e2e,
                 "gpu_launches": launches_per_step * args.steps,
-                "clocks": clk.summary()}
+                "clocks": clk.summary(), "variants": variants}
         print(json.dumps(line), flush=True)
     eng.close()
     if ws > 1:
@@ -364,14 +384,51 @@ def run_ours(args):
     return line
 
 
+def run_kernels(args):
+    """Profiling case: the cfg1 series with every length divided by --scale,
+    then --iters SIRT iterations (forward splat, residual, back-projection
+    with update per iteration) after the weight passes.  Prints timings
+    only; not a bench line."""
+    import torch
+
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+    build.build_lib()
+    cfg = synth.config("cfg1", args.scale)
+    coeff = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    eng = T.Engine(0)
+    eng.set_problem(nx, ny, nt, th, coeff, T.LAYOUT_Y)
+    proj = make_series(eng, torch, cfg, coeff)
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    eng.sirt(proj, vol, 1, cfg.gamma)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    eng.sirt(proj, vol, args.iters, cfg.gamma)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, args.iters)
+    print(json.dumps({"case": f"cfg1/{args.scale}", "proj": [nt, ny, nx],
+                      "volume": [nx, ny, th], "iters": args.iters,
+                      "ms_per_iter": ms}), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--kernels", action="store_true",
+                    help="profiling case only (see run_kernels)")
+    ap.add_argument("--scale", type=int, default=2)
+    ap.add_argument("--iters", type=int, default=2)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernels:
+        run_kernels(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -218,6 +218,10 @@ def test_errors_are_reported(engine):
     engine.set_problem(16, 8, 1, 4, np.array([[0, 1, 0, 0, 0, 0, 1, 0.]]))
     with pytest.raises(T.TiltRecError):
         engine.backproject(torch.zeros(1, device="cuda"), torch.zeros(1, device="cuda"), 3, 5)
+    # A tile window wider than the kernels' Q9.23 coordinates address.
+    with pytest.raises(T.TiltRecError) as e:
+        engine.set_problem(64, 8, 1, 4, np.array([[0, 20, 0, 0, 0, 0, 1, 0.]]))
+    assert e.value.status == -7  # TR_ERR_UNSUPPORTED
     small = T.Engine(0, hbm_budget=1024)
     small.set_problem(64, 64, 4, 8, np.tile([[0, 1, 0, 0, 0, 0, 1, 0.]], (4, 1)))
     with pytest.raises(T.TiltRecError) as e:
