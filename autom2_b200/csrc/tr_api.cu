@@ -603,6 +603,66 @@ tr_status tr_forward_project(tr_ctx *c, const float *vol, int z0, int nz, float 
   return TR_OK;
 }
 
+tr_status tr_forward_project_tilts(tr_ctx *c, const float *vol, int z0, int nz, int t0,
+                                   int ntilts, float *val, float *wt, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!vol || !val || z0 < 0 || nz < 1 || z0 + nz > c->th || t0 < 0 || ntilts < 1 ||
+      t0 + ntilts > c->nt)
+    return fail(c, TR_ERR_ARG, "bad forward-projection arguments (z0=%d nz=%d t0=%d nt=%d)",
+                z0, nz, t0, ntilts);
+  FpArgs a = fp_args(c, vol, z0, nz, val, 0, ntilts);
+  a.geo = c->geo_d + t0;
+  TR_CUDA(c, launch_fp(c->sep, a, (cudaStream_t)stream));
+  if (wt) {
+    FpArgs w = fp_args(c, nullptr, z0, nz, wt, 0, ntilts);
+    w.geo = c->geo_d + t0;
+    TR_CUDA(c, launch_fp(c->sep, w, (cudaStream_t)stream));
+  }
+  return TR_OK;
+}
+
+tr_status tr_residual(tr_ctx *c, const float *proj, float *val, const float *wt, int ntilts,
+                      void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !val || !wt || ntilts < 1 || ntilts > c->nt)
+    return fail(c, TR_ERR_ARG, "bad residual arguments (ntilts=%d)", ntilts);
+  TR_CUDA(c, launch_resid(proj, val, wt, (size_t)c->nx * c->ny * ntilts, c->nsm,
+                          (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_sirt_update(tr_ctx *c, const float *resid, float *vol, int z0, int nz,
+                         float gamma, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!resid || !vol || z0 < 0 || nz < 1 || z0 + nz > c->th)
+    return fail(c, TR_ERR_ARG, "bad SIRT update arguments (z0=%d nz=%d)", z0, nz);
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((st = ensure_wtvol(c, s))) return st;
+  BpArgs b = bp_args(c, vol, z0, nz, resid, 0, c->nt, gamma);
+  // The cached weights cover the whole volume; view the same sections.
+  b.wtvol = c->wtvol_d + (c->layout == TR_LAYOUT_Y ? (size_t)z0 * c->nx
+                                                   : (size_t)z0 * c->nx * c->ny);
+  TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
+  return TR_OK;
+}
+
+tr_status tr_sart_update(tr_ctx *c, const float *resid_plane, int tilt, float *vol, int z0,
+                         int nz, float gamma, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!resid_plane || !vol || tilt < 0 || tilt >= c->nt || z0 < 0 || nz < 1 ||
+      z0 + nz > c->th)
+    return fail(c, TR_ERR_ARG, "bad SART update arguments (tilt=%d z0=%d nz=%d)", tilt, z0,
+                nz);
+  BpArgs b = bp_args(c, vol, z0, nz, resid_plane, 0, 1, gamma);
+  b.geo = c->geo_d + tilt;
+  TR_CUDA(c, run_bp(c, BP_NORM, b, (cudaStream_t)stream));
+  return TR_OK;
+}
+
 tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gamma,
                   void *stream) {
   tr_status st = need_problem(c);

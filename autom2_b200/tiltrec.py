@@ -94,6 +94,10 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_sart.argtypes = [vp, vp, vp, i, f, vp]
     lib.tr_wbp.argtypes = [vp, vp, vp, vp]
     lib.tr_reconstruct_host.argtypes = [vp, i, vp, vp, i, f]
+    lib.tr_forward_project_tilts.argtypes = [vp, vp, i, i, i, i, vp, vp, vp]
+    lib.tr_residual.argtypes = [vp, vp, vp, vp, i, vp]
+    lib.tr_sirt_update.argtypes = [vp, vp, vp, i, i, f, vp]
+    lib.tr_sart_update.argtypes = [vp, vp, i, vp, i, i, f, vp]
     lib.tr_quantize.argtypes = [vp, vp, i, vp, vp, vp]
     lib.tr_backproject_lp.argtypes = [vp, vp, i, vp, vp, i, i, vp]
     lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
@@ -212,6 +216,31 @@ class Engine:
         self._check(self.lib.tr_forward_project(self.h, _ptr(vol), z0, nz, _ptr(val),
                                                 _ptr(wt), _stream(self.device)),
                     "tr_forward_project")
+
+    def forward_project_tilts(self, vol, t0, ntilts, val, wt=None, z0=0, nz=None):
+        """Forward projection of tilts [t0, t0+ntilts); val/wt hold those
+        tilts' planes only."""
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_forward_project_tilts(self.h, _ptr(vol), z0, nz, t0, ntilts,
+                                                      _ptr(val), _ptr(wt),
+                                                      _stream(self.device)),
+                    "tr_forward_project_tilts")
+
+    def residual(self, proj, val, wt):
+        """val <- proj - val/wt (val where wt == 0), over proj.shape[0]
+        planes."""
+        self._check(self.lib.tr_residual(self.h, _ptr(proj), _ptr(val), _ptr(wt),
+                                         proj.shape[0], _stream(self.device)), "tr_residual")
+
+    def sirt_update(self, resid, vol, gamma, z0=0, nz=None):
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_sirt_update(self.h, _ptr(resid), _ptr(vol), z0, nz, gamma,
+                                            _stream(self.device)), "tr_sirt_update")
+
+    def sart_update(self, resid_plane, tilt, vol, gamma, z0=0, nz=None):
+        nz = self.shape[3] - z0 if nz is None else nz
+        self._check(self.lib.tr_sart_update(self.h, _ptr(resid_plane), tilt, _ptr(vol), z0, nz,
+                                            gamma, _stream(self.device)), "tr_sart_update")
 
     def sirt(self, proj, vol, iters, gamma):
         self._check(self.lib.tr_sirt(self.h, _ptr(proj), _ptr(vol), iters, gamma,

@@ -135,6 +135,36 @@ tr_status tr_sirt(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
 tr_status tr_sart(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
                   int iters, float gamma, void *stream);
 
+/* Building blocks of SIRT / SART for callers that own the iteration, e.g.
+ * one rank per GPU holding a z-slab of the volume and summing the forward
+ * projections of all slabs between the two passes, as TiltRecZ-mpi does
+ * with MPI_Allreduce (main-mpiz.cpp:548-601).
+ *
+ * tr_forward_project_tilts: as tr_forward_project for tilts
+ * [t0, t0+ntilts) only; val_dev / wt_dev point at tilt t0's plane. */
+tr_status tr_forward_project_tilts(tr_ctx *ctx, const float *vol_dev, int z0,
+                                   int nz, int t0, int ntilts, float *val_dev,
+                                   float *wt_dev, void *stream);
+
+/* Residual in place over ntilts planes: val <- proj - (wt != 0 ? val/wt : val)
+ * (main-mpi.cpp:640-647). */
+tr_status tr_residual(tr_ctx *ctx, const float *proj_dev, float *val_dev,
+                      const float *wt_dev, int ntilts, void *stream);
+
+/* SIRT update from the residuals of all tilts on sections [z0, z0+nz):
+ * vol += gamma * (sum_t s) / (sum_t c) where sum_t c != 0, the voxel weight
+ * sums cached per geometry.  UpdateWeightsByProjDiff + UpdateVolumeByWeights
+ * (main-mpi.cpp:526-576; main-mpiz.cpp:453-501). */
+tr_status tr_sirt_update(tr_ctx *ctx, const float *resid_dev, float *vol_dev,
+                         int z0, int nz, float gamma, void *stream);
+
+/* SART update of one tilt from its residual plane on sections [z0, z0+nz):
+ * vol += gamma * s/c where c != 0.  UpdateVolumeByProjDiff
+ * (main-mpi.cpp:492-524; main-mpiz.cpp:419-451). */
+tr_status tr_sart_update(tr_ctx *ctx, const float *resid_plane_dev, int tilt,
+                         float *vol_dev, int z0, int nz, float gamma,
+                         void *stream);
+
 /* WBP: filter proj_dev in place, then vol += back-projection.
  * main-mpi.cpp:841-846 (ApplyFilterInplace mode 2 + BackProject), CuFBP with
  * filterMode 2 (recon_y.cuh:28). */

@@ -1,0 +1,25 @@
+"""Multi-rank reconstruction through the sm_100a kernels: two ranks (two
+processes, gloo collectives staged through host memory) share the one GPU
+and run autom2_b200.shard with the Engine as the per-rank operator.  The
+ranks' kernels never wait on one another; only the host-side sums join
+them.  Bar: the plain FP32 one, relative L2 1e-5 against the oracle's
+whole-volume reconstruction."""
+import numpy as np
+import pytest
+
+import oracle as O
+from test_shard import _cases, _whole, run_ranks
+
+pytestmark = pytest.mark.gpu
+
+
+def test_two_ranks_on_the_gpu_match_whole_volume(engine, restatement, tmp_path):
+    R = restatement
+    cases = _cases(R)
+    run_ranks(cases, tmp_path, use_gpu=True)
+    for name, c in cases.items():
+        want = _whole(R, c)
+        for rank in range(2):
+            got = np.load(tmp_path / f"{name}_{rank}.npy")
+            err = O.rel_l2(got, want)
+            assert err < 1e-5, (name, rank, err)
