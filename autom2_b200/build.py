@@ -24,7 +24,7 @@ BINDIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIBDIR, "libtiltrec_b200.so")
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["tr_kernels.cu", "tr_filter.cu", "tr_api.cu", "tr_static.cu"]
+CU_SOURCES = ["tr_kernels.cu", "tr_filter.cu", "tr_api.cu", "tr_static.cu", "tr_sched.cu"]
 CLI_SOURCES = ["mrc_io.cpp", "tiltrec_cli.cpp"]
 
 
@@ -51,7 +51,8 @@ def _run(cmd: list[str]) -> None:
 
 def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES]
-    deps = srcs + [os.path.join(CSRC, "tr_internal.cuh"),
+    deps = srcs + [os.path.join(CSRC, "tr_internal.cuh"), os.path.join(CSRC, "tr_geom.h"),
+                   os.path.join(CSRC, "tr_filter_host.h"),
                    os.path.join(INCLUDE, "tiltrec_b200.h")]
     if not force and _newer(LIB, deps):
         return LIB

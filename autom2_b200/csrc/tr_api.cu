@@ -12,28 +12,10 @@
 #include <vector>
 
 #include "tiltrec_b200.h"
+#include "tr_filter_host.h"
+#include "tr_geom.h"
 #include "tr_internal.cuh"
 
-namespace trb {
-cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
-cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
-cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
-                         int nsm, cudaStream_t s);
-cudaError_t launch_quantize(const float *p, size_t plane, int nt, int dtype, void *out,
-                            float *scale, unsigned *maxbits, int nsm, cudaStream_t s);
-cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const float *val,
-                            const float *wt, size_t plane, int nt, int rdtype, void *r,
-                            const float *rs, int nsm, cudaStream_t s);
-struct FilterArgs {
-  float *rows;
-  long long nrows;
-  int nx, n_pad;
-  int log2m;
-  const float2 *ghat;
-  const float2 *tw;
-};
-cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
-}  // namespace trb
 
 using namespace trb;
 
@@ -65,6 +47,7 @@ struct tr_ctx {
   float *val_d = nullptr, *wt_d = nullptr, *wtvol_d = nullptr;
   void *res16_d = nullptr;      // 16-bit SIRT residual [ntilt][ny][nx]
   unsigned *maxbits_d = nullptr;  // per-tilt |p| maxima for tr_quantize
+  float *rscale_d = nullptr;      // per-tilt scales of the FP16 SIRT residual
   bool wt_ready = false, wtvol_ready = false;
   int filt_nx = 0, filt_npad = 0, filt_log2m = 0;
   float2 *ghat_d = nullptr, *tw_d = nullptr;
@@ -132,6 +115,7 @@ void release_problem(tr_ctx *c) {
   scratch_free(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float));
   scratch_free(c, (void **)&c->res16_d, proj_elems(c) * 2);
   scratch_free(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt);
+  scratch_free(c, (void **)&c->rscale_d, sizeof(float) * c->nt);
   if (c->geo_d) {
     cudaFree(c->geo_d);
     c->geo_d = nullptr;
@@ -226,93 +210,26 @@ FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
   return a;
 }
 
-// Iterative radix-2 FFT in double (host), forward sign -1.
-void fft_host(std::vector<std::complex<double>> &x) {
-  const size_t n = x.size();
-  for (size_t i = 1, j = 0; i < n; ++i) {
-    size_t bit = n >> 1;
-    for (; j & bit; bit >>= 1) j ^= bit;
-    j ^= bit;
-    if (i < j) std::swap(x[i], x[j]);
-  }
-  for (size_t len = 2; len <= n; len <<= 1) {
-    const double ang = -2.0 * M_PI / (double)len;
-    for (size_t i = 0; i < n; i += len)
-      for (size_t k = 0; k < len / 2; ++k) {
-        const std::complex<double> w(cos(ang * k), sin(ang * k));
-        const std::complex<double> u = x[i + k], v = x[i + k + len / 2] * w;
-        x[i + k] = u + v;
-        x[i + k + len / 2] = u - v;
-      }
-  }
-}
-
 // Kernel spectrum of the R-weighting filter for rows of nx samples.
 tr_status build_filter(tr_ctx *c, int nx) {
   if (c->filt_nx == nx && c->ghat_d) return TR_OK;
-  const int N = nx + nx / 10;
-  int log2m = 1;
-  while ((1 << log2m) < N + nx - 1) ++log2m;
-  const int M = 1 << log2m;
-  if ((size_t)M * sizeof(float2) > kSmemMax)
-    return fail(c, TR_ERR_UNSUPPORTED, "row length %d needs an FFT of %d points", nx, M);
-  // Weights exactly as filter_prj.cpp:694-723 forms them (float arithmetic).
-  const int r = (int)floor((float)N * 0.05f);
-  const float sg = (float)N * 0.5f;
-  const int nb = N / 2 + 1;
-  std::vector<double> W(nb);
-  for (int k = 0; k < nb; ++k) {
-    if (k == 0)
-      W[k] = 0.2;
-    else if (k <= r)
-      W[k] = k;
-    else
-      W[k] = (double)(float)r * (double)expf(-(float)((k - r) * (k - r)) / (sg * sg));
-  }
-  // h[d] = sum over the Hermitian-extended spectrum of W cos(2 pi k d / N).
-  std::vector<double> cs(N), h(N);
-  for (int j = 0; j < N; ++j) cs[j] = cos(2.0 * M_PI * j / N);
-  const int kmax = (N % 2 == 0) ? N / 2 - 1 : (N - 1) / 2;
-  for (int d = 0; d < N; ++d) {
-    double acc = W[0];
-    for (int k = 1; k <= kmax; ++k) acc += 2.0 * W[k] * cs[(long long)k * d % N];
-    if (N % 2 == 0) acc += (d % 2 == 0) ? W[N / 2] : -W[N / 2];
-    h[d] = acc;
-  }
-  std::vector<std::complex<double>> g(M, 0.0);
-  for (int e = -(N - 1); e <= nx - 1; ++e) g[(e % M + M) % M] = h[(e % N + N) % N];
-  fft_host(g);
-  std::vector<float2> ghat(M), tw(M / 2);
-  const double scale = 1.0 / ((double)M * nx);
-  for (int i = 0; i < M; ++i) {
-    int br = 0;
-    for (int b = 0; b < log2m; ++b) br |= ((i >> b) & 1) << (log2m - 1 - b);
-    ghat[i] = make_float2((float)(g[br].real() * scale), (float)(g[br].imag() * scale));
-  }
-  for (int k = 0; k < M / 2; ++k)
-    tw[k] = make_float2((float)cos(2.0 * M_PI * k / M), (float)-sin(2.0 * M_PI * k / M));
+  RweightSpectrum sp;
+  if (!rweight_spectrum(nx, kSmemMax, &sp))
+    return fail(c, TR_ERR_UNSUPPORTED, "row length %d needs an FFT of %d points", nx,
+                1 << sp.log2m);
+  const int M = 1 << sp.log2m;
   if (c->ghat_d) scratch_free(c, (void **)&c->ghat_d, sizeof(float2) << c->filt_log2m);
   if (c->tw_d) scratch_free(c, (void **)&c->tw_d, sizeof(float2) << (c->filt_log2m - 1));
   tr_status s = scratch_alloc(c, (void **)&c->ghat_d, sizeof(float2) * M, "filter spectrum");
   if (s) return s;
   s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * (M / 2), "filter twiddles");
   if (s) return s;
-  TR_CUDA(c, cudaMemcpy(c->ghat_d, ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-  TR_CUDA(c, cudaMemcpy(c->tw_d, tw.data(), sizeof(float2) * (M / 2), cudaMemcpyHostToDevice));
+  TR_CUDA(c, cudaMemcpy(c->ghat_d, sp.ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+  TR_CUDA(c, cudaMemcpy(c->tw_d, sp.tw.data(), sizeof(float2) * (M / 2), cudaMemcpyHostToDevice));
   c->filt_nx = nx;
-  c->filt_npad = N;
-  c->filt_log2m = log2m;
+  c->filt_npad = sp.npad;
+  c->filt_log2m = sp.log2m;
   return TR_OK;
-}
-
-// Most voxels of one forward-projection tile that can add to one window entry:
-// along x a row of voxels steps the detector column by |a1|, so at most
-// floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their lower
-// column at q-1 or q; every (y, z) row of the tile may contribute.
-float fp_entry_bound(double min_a1) {
-  double nx = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
-  nx = std::min(nx, (double)kFX);
-  return (float)(nx * kTY * kFTZ);
 }
 
 // Validates coefficients, derives the fixed-point steps and the per-tile
@@ -321,53 +238,22 @@ float fp_entry_bound(double min_a1) {
 tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   const int nt = c->nt;
   std::vector<TiltGeo> g(nt);
-  bool sep = true;
-  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
-  const double two32 = 4294967296.0;
-  const double ext = std::max(std::max(c->nx, c->ny), c->th) + 64.0;
-  for (int t = 0; t < nt; ++t) {
-    const double *k = coeff8 + 8 * (size_t)t;
-    for (int i = 0; i < 4; ++i) {
-      g[t].a[i] = k[i];
-      g[t].b[i] = k[4 + i];
-      if (!std::isfinite(k[i]) || !std::isfinite(k[4 + i]))
-        return fail(c, TR_ERR_ARG, "non-finite coefficient at tilt %d", t);
-    }
-    for (int i = 0; i < 3; ++i) {
-      if (fabs(k[1 + i]) > 1024.0 || fabs(k[5 + i]) > 1024.0)
-        return fail(c, TR_ERR_UNSUPPORTED, "coefficient magnitude above 1024 at tilt %d", t);
-      g[t].A[i] = llrint(k[1 + i] * two32);
-      g[t].B[i] = llrint(k[5 + i] * two32);
-    }
-    // Detector coordinates must stay far inside the int range of the table
-    // origins for every voxel of the volume.
-    const double reach_u = fabs(k[0]) + (fabs(k[1]) + fabs(k[2]) + fabs(k[3])) * 2 * ext;
-    const double reach_v = fabs(k[4]) + (fabs(k[5]) + fabs(k[6]) + fabs(k[7])) * 2 * ext;
-    if (reach_u > 1.0e9 || reach_v > 1.0e9)
-      return fail(c, TR_ERR_UNSUPPORTED, "detector coordinates out of range at tilt %d", t);
-    if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
-    min_a1 = std::min(min_a1, fabs(k[1]));
-    span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
-                                  fabs(k[3]) * (kTZ - 1));
-    span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
-                                  fabs(k[7]) * (kTZ - 1));
-    fspan_u = std::max(fspan_u, fabs(k[1]) * (kFX - 1) + fabs(k[2]) * (kTY - 1) +
-                                    fabs(k[3]) * (kFTZ - 1));
-    fspan_v = std::max(fspan_v, fabs(k[5]) * (kFX - 1) + fabs(k[6]) * (kTY - 1) +
-                                    fabs(k[7]) * (kFTZ - 1));
+  GeomInfo gi;
+  int bad = -1;
+  switch (derive_geometry(coeff8, nt, c->nx, c->ny, c->th, kSmemMax, g.data(), &gi, &bad)) {
+    case GEOM_OK: break;
+    case GEOM_NONFINITE: return fail(c, TR_ERR_ARG, "non-finite coefficient at tilt %d", bad);
+    case GEOM_MAGNITUDE:
+      return fail(c, TR_ERR_UNSUPPORTED, "coefficient magnitude above 1024 at tilt %d", bad);
+    case GEOM_RANGE:
+      return fail(c, TR_ERR_UNSUPPORTED, "detector coordinates out of range at tilt %d", bad);
+    case GEOM_SMEM:
+      return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds shared memory",
+                  gi.ffw, gi.ffh);
+    default:
+      return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds %d",
+                  std::max(gi.fw, gi.ffw), std::max(gi.fh, gi.ffh), kMaxWindow);
   }
-  const int fw = (int)ceil(span_u) + 4;
-  const int fh = sep ? kTY : (int)ceil(span_v) + 5;
-  const int ffw = (int)ceil(fspan_u) + 4;
-  const int ffh = sep ? kTY : (int)ceil(fspan_v) + 5;
-  const size_t ent_bp = (size_t)fw * fh * sizeof(float2);
-  const size_t ent_fp = (size_t)ffw * ffh * sizeof(float);
-  if (ent_bp > kSmemMax || ent_fp > kSmemMax)
-    return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds shared memory",
-                ffw, ffh);
-  if (std::max(std::max(fw, fh), std::max(ffw, ffh)) > kMaxWindow)
-    return fail(c, TR_ERR_UNSUPPORTED, "detector window %dx%d per tile exceeds %d",
-                std::max(fw, ffw), std::max(fh, ffh), kMaxWindow);
   if (s) {
     TR_CUDA(c, cudaMemcpyAsync(c->geo_d, g.data(), sizeof(TiltGeo) * nt,
                                cudaMemcpyHostToDevice, s));
@@ -375,14 +261,14 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   } else {
     TR_CUDA(c, cudaMemcpy(c->geo_d, g.data(), sizeof(TiltGeo) * nt, cudaMemcpyHostToDevice));
   }
-  c->fw = fw;
-  c->fh = fh;
-  c->ffw = ffw;
-  c->ffh = ffh;
-  c->fp_nbound = fp_entry_bound(min_a1);
-  c->sep = sep;
-  c->chunk_bp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemBp / ent_bp));
-  c->chunk_fp = (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kSmemFp / ent_fp));
+  c->fw = gi.fw;
+  c->fh = gi.fh;
+  c->ffw = gi.ffw;
+  c->ffh = gi.ffh;
+  c->fp_nbound = gi.nbound;
+  c->sep = gi.sep;
+  c->chunk_bp = chunk_for(kSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
+  c->chunk_fp = chunk_for(kSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
   c->wt_ready = c->wtvol_ready = false;
   return TR_OK;
 }
@@ -746,7 +632,7 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
     return d == TR_DTYPE_F32 || d == TR_DTYPE_F16 || d == TR_DTYPE_BF16;
   };
   if (!proj || !vol || iters < 0 || !ok_dtype(pdtype) || !ok_dtype(rdtype) ||
-      (pdtype != TR_DTYPE_F32 && !scale) || (rdtype == TR_DTYPE_F16 && !scale))
+      (pdtype != TR_DTYPE_F32 && !scale))
     return fail(c, TR_ERR_ARG, "bad SIRT arguments (proj dtype %d, residual dtype %d)",
                 pdtype, rdtype);
   cudaStream_t s = (cudaStream_t)stream;
@@ -755,17 +641,33 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
   if (rdtype != TR_DTYPE_F32 &&
       (st = scratch_alloc(c, &c->res16_d, pn * 2, "16-bit residual")))
     return st;
+  if (rdtype == TR_DTYPE_F16 &&
+      ((st = scratch_alloc(c, (void **)&c->rscale_d, sizeof(float) * c->nt,
+                           "residual scales")) ||
+       (st = scratch_alloc(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt,
+                           "per-tilt maxima"))))
+    return st;
   if ((st = ensure_wt(c, s))) return st;
   if ((st = ensure_wtvol(c, s))) return st;
   const float *ps = pdtype == TR_DTYPE_F32 ? nullptr : scale;
-  const float *rs = rdtype == TR_DTYPE_F16 ? scale : nullptr;
   void *res = rdtype == TR_DTYPE_F32 ? (void *)c->val_d : c->res16_d;
+  const float *rs = rdtype == TR_DTYPE_F16 ? c->rscale_d : nullptr;
   for (int it = 0; it < iters; ++it) {
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
     FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
     TR_CUDA(c, launch_fp(c->sep, f, s));
-    TR_CUDA(c, launch_resid_lp(proj, pdtype, ps, c->val_d, c->wt_d, plane, c->nt, rdtype, res,
-                               rs, c->nsm, s));
+    if (rdtype == TR_DTYPE_F16) {
+      // The residual's range is not the stack's (a WBP start, for one, makes
+      // it larger): form it in FP32, then store it with its own per-tilt
+      // power-of-two scales.
+      TR_CUDA(c, launch_resid_lp(proj, pdtype, ps, c->val_d, c->wt_d, plane, c->nt,
+                                 TR_DTYPE_F32, c->val_d, nullptr, c->nsm, s));
+      TR_CUDA(c, launch_quantize(c->val_d, plane, c->nt, TR_DTYPE_F16, c->res16_d, c->rscale_d,
+                                 c->maxbits_d, c->nsm, s));
+    } else {
+      TR_CUDA(c, launch_resid_lp(proj, pdtype, ps, c->val_d, c->wt_d, plane, c->nt, rdtype,
+                                 res, nullptr, c->nsm, s));
+    }
     BpArgs b = bp_args(c, vol, 0, c->th, (const float *)res, 0, c->nt, gamma);
     b.img.dtype = rdtype;
     b.img.scale = rs;

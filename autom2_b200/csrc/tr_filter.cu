@@ -21,16 +21,9 @@
 // rows at once because the kernel is real.
 #include <cuda_runtime.h>
 
-namespace trb {
+#include "tr_internal.cuh"
 
-struct FilterArgs {
-  float *rows;          // [nrows][nx], filtered in place
-  long long nrows;
-  int nx, n_pad;        // row length and the reference's padded length N
-  int log2m;            // M = 1 << log2m
-  const float2 *ghat;   // [M] kernel spectrum, bit-reversed, scaled
-  const float2 *tw;     // [M/2] e^{-2 pi i k / M}
-};
+namespace trb {
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);

@@ -1,0 +1,101 @@
+// Host-side derivation of the kernels' per-tilt geometry: the Q32.32 voxel
+// steps, the per-tile detector window sizes and the forward-projection
+// fixed-point bound, shared by the context, the no-allocation entry point and
+// the batch scheduler.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+
+#include "tr_internal.cuh"
+
+namespace trb {
+
+struct GeomInfo {
+  int fw, fh;      // back-projection tile window (columns, rows)
+  int ffw, ffh;    // forward-projection tile window
+  float nbound;    // most voxel contributions one forward window entry collects
+  bool sep;        // every tilt has b1 = b3 = 0, b2 = 1 (separable rows)
+};
+
+enum GeomStatus {
+  GEOM_OK = 0,
+  GEOM_NONFINITE,   // a coefficient is NaN or infinite
+  GEOM_MAGNITUDE,   // a slope above 1024
+  GEOM_RANGE,       // detector coordinates beyond the int range of the windows
+  GEOM_SMEM,        // one tilt's window exceeds smem_max
+  GEOM_WINDOW,      // a window side exceeds kMaxWindow
+};
+
+// Most voxels of one forward-projection tile that can add to one window entry:
+// along x a row of voxels steps the detector column by |a1|, so at most
+// floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their lower
+// column at q-1 or q; every (y, z) row of the tile may contribute.
+inline float fp_entry_bound(double min_a1) {
+  double n = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
+  n = std::min(n, (double)kFX);
+  return (float)(n * kTY * kFTZ);
+}
+
+// Fills g[0..nt) and *out from [nt][8] coefficients; *bad_tilt names the
+// offending tilt for the per-tilt failures.
+inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
+                           size_t smem_max, TiltGeo *g, GeomInfo *out, int *bad_tilt) {
+  bool sep = true;
+  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
+  const double two32 = 4294967296.0;
+  const double ext = std::max(std::max(nx, ny), th) + 64.0;
+  *bad_tilt = -1;
+  for (int t = 0; t < nt; ++t) {
+    const double *k = coeff8 + 8 * (size_t)t;
+    *bad_tilt = t;
+    for (int i = 0; i < 4; ++i) {
+      if (!std::isfinite(k[i]) || !std::isfinite(k[4 + i])) return GEOM_NONFINITE;
+      g[t].a[i] = k[i];
+      g[t].b[i] = k[4 + i];
+    }
+    for (int i = 0; i < 3; ++i) {
+      if (std::fabs(k[1 + i]) > 1024.0 || std::fabs(k[5 + i]) > 1024.0) return GEOM_MAGNITUDE;
+      g[t].A[i] = std::llrint(k[1 + i] * two32);
+      g[t].B[i] = std::llrint(k[5 + i] * two32);
+    }
+    // Detector coordinates must stay far inside the int range of the window
+    // origins for every voxel of the volume.
+    const double reach_u =
+        std::fabs(k[0]) + (std::fabs(k[1]) + std::fabs(k[2]) + std::fabs(k[3])) * 2 * ext;
+    const double reach_v =
+        std::fabs(k[4]) + (std::fabs(k[5]) + std::fabs(k[6]) + std::fabs(k[7])) * 2 * ext;
+    if (reach_u > 1.0e9 || reach_v > 1.0e9) return GEOM_RANGE;
+    if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
+    min_a1 = std::min(min_a1, std::fabs(k[1]));
+    span_u = std::max(span_u, std::fabs(k[1]) * (kTX - 1) + std::fabs(k[2]) * (kTY - 1) +
+                                  std::fabs(k[3]) * (kTZ - 1));
+    span_v = std::max(span_v, std::fabs(k[5]) * (kTX - 1) + std::fabs(k[6]) * (kTY - 1) +
+                                  std::fabs(k[7]) * (kTZ - 1));
+    fspan_u = std::max(fspan_u, std::fabs(k[1]) * (kFX - 1) + std::fabs(k[2]) * (kTY - 1) +
+                                    std::fabs(k[3]) * (kFTZ - 1));
+    fspan_v = std::max(fspan_v, std::fabs(k[5]) * (kFX - 1) + std::fabs(k[6]) * (kTY - 1) +
+                                    std::fabs(k[7]) * (kFTZ - 1));
+  }
+  *bad_tilt = -1;
+  out->fw = (int)std::ceil(span_u) + 4;
+  out->fh = sep ? kTY : (int)std::ceil(span_v) + 5;
+  out->ffw = (int)std::ceil(fspan_u) + 4;
+  out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5;
+  out->sep = sep;
+  out->nbound = fp_entry_bound(min_a1);
+  const size_t ent_bp = (size_t)out->fw * out->fh * sizeof(float2);
+  const size_t ent_fp = (size_t)out->ffw * out->ffh * sizeof(float);
+  if (ent_bp > smem_max || ent_fp > smem_max) return GEOM_SMEM;
+  if (std::max(std::max(out->fw, out->fh), std::max(out->ffw, out->ffh)) > kMaxWindow)
+    return GEOM_WINDOW;
+  return GEOM_OK;
+}
+
+// Tilts staged per chunk when one tilt's window takes `entry` bytes of a
+// `budget`-byte table.
+inline int chunk_for(size_t budget, size_t entry) {
+  return (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, budget / entry));
+}
+
+}  // namespace trb

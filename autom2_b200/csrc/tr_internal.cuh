@@ -1,6 +1,8 @@
 // Internal definitions shared by the TiltRec B200 kernels and the C-ABI.
 #pragma once
 
+#include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -109,5 +111,96 @@ struct SepRow {
   int y0;
   float dy;
 };
+
+// R-weighting filter of rows in place (tr_filter.cu).
+struct FilterArgs {
+  float *rows;          // [nrows][nx], filtered in place
+  long long nrows;
+  int nx, n_pad;        // row length and the reference's padded length N
+  int log2m;            // M = 1 << log2m
+  const float2 *ghat;   // [M] kernel spectrum, bit-reversed, scaled
+  const float2 *tw;     // [M/2] e^{-2 pi i k / M}
+};
+
+// ------------------------------------------------------------ batched steps
+//
+// A batch step runs the same stage for many jobs in one launch: a table in
+// device memory lists work items; the persistent forward and back-projection
+// kernels pull tiles of all items from one atomic counter.  The same launches
+// (captured once in a CUDA graph) serve every step: only the table changes.
+
+constexpr int kBatchMaxItems = 256;  // per item kind
+
+struct __align__(64) BatchBp {
+  CUtensorMap map;  // TMA descriptor of the item's image stack
+  BpArgs a;         // chunk / tma_* laid out for the step's shared budget
+  int mode, sep;
+  int gx, gy, gz;   // tile grid
+  long long first;  // global index of the item's first tile
+};
+
+struct BatchFp {
+  FpArgs a;
+  int sep;
+  int gx, gy, gz;
+  long long first;
+};
+
+struct BatchRes {       // r = p*ps[t] - val/wt, stored as rdtype in units of rs[t]
+  const void *p;
+  const float *ps;
+  const float *val, *wt;
+  void *r;
+  const float *rs;
+  unsigned long long plane;
+  int nt, pdtype, rdtype;
+  // FP16 residuals: r is FP32 (over val), then stored at q as FP16 with
+  // per-tilt power-of-two scales qscale from the maxima qmax (zeroed by the
+  // zero stage); q == nullptr: none
+  __half *q;
+  float *qscale;
+  unsigned *qmax;
+};
+
+struct BatchZero {
+  float *p;
+  unsigned long long n;
+};
+
+struct BatchHeader {
+  int nbp, nfp, nres, nzero;
+  int *err;                             // abort word of the step's waits, reset by zero
+  long long bp_tiles, fp_tiles;
+  unsigned long long bp_next, fp_next;  // work counters, reset by the zero stage
+};
+
+// Device table: header, then the item arrays at fixed offsets.
+struct BatchTable {
+  BatchHeader h;
+  BatchBp bp[kBatchMaxItems];
+  BatchFp fp[kBatchMaxItems];
+  BatchRes res[kBatchMaxItems];
+  BatchZero zero[kBatchMaxItems];
+};
+
+// ------------------------------------------------------------ launchers
+// (tr_kernels.cu, tr_filter.cu)
+
+cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
+cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
+cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n, int nsm,
+                         cudaStream_t s);
+cudaError_t launch_quantize(const float *p, size_t plane, int nt, int dtype, void *out,
+                            float *scale, unsigned *maxbits, int nsm, cudaStream_t s);
+cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const float *val,
+                            const float *wt, size_t plane, int nt, int rdtype, void *r,
+                            const float *rs, int nsm, cudaStream_t s);
+cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
+dim3 bp_tile_grid(const VolView &v);
+dim3 fp_tile_grid(const VolView &v);
+bool batch_bp_layout(const BpArgs &a0, bool sep, size_t budget, BatchBp *out, size_t *smem);
+int batch_occupancy(int rdtype, size_t smem_bp, size_t smem_fp, int *fp_per_sm);
+cudaError_t launch_batch_step(BatchTable *T, int rdtype, int grid_fp, int grid_bp,
+                              size_t smem_fp, size_t smem_bp, int nsm, cudaStream_t s);
 
 }  // namespace trb

@@ -190,18 +190,13 @@ struct EntryWalk {
 };
 
 // Interpolation of one staged chunk of tilts into the thread's accumulators.
-// Adds val to a voxel accumulator; with KAHAN the running compensation c
-// carries the low-order bits lost by each addition (compensated summation).
-template <bool KAHAN>
-__device__ __forceinline__ void acc_add(float &acc, float &c, float val) {
-  if (KAHAN) {
-    const float y = val - c;
-    const float t = acc + y;
-    c = (t - acc) - y;
-    acc = t;
-  } else {
-    acc += val;
-  }
+// Compensated (Kahan) addition of val to a voxel accumulator: the running
+// compensation c carries the low-order bits each addition loses.
+__device__ __forceinline__ void kahan_add(float &acc, float &c, float val) {
+  const float y = val - c;
+  const float t = acc + y;
+  c = (t - acc) - y;
+  acc = t;
 }
 
 // Window coordinates inside the z loop run in Q9.23 (32-bit): the integer
@@ -221,6 +216,14 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
                                               const TileTilt *tt, const TiltGeo *geo,
                                               int nc, int per, int fw, int pny,
                                               int lane, int wy, int wz) {
+  // KAHAN: the chunk's tilts (at most kMaxChunk) sum into a plain partial,
+  // which joins the voxel's total by one compensated addition per chunk.
+  float part[kNV];
+  float(&sum)[kNV] = KAHAN ? part : acc;
+  if (KAHAN) {
+#pragma unroll
+    for (int k = 0; k < kNV; ++k) part[k] = 0.f;
+  }
   for (int i = 0; i < nc; ++i) {
     const TiltGeo &g = geo[i];
     const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
@@ -232,7 +235,7 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
 #pragma unroll
       for (int k = 0; k < kNV; ++k) {
         const float2 t = T[u >> 23];
-        acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac23(u), t.y, t.x));
+        sum[k] += fmaf(one_plus_frac23(u), t.y, t.x);
         u += du;
       }
     } else {
@@ -251,7 +254,7 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
           const float f = one_plus_frac23(u);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
           const float val = fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
-          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) acc_add<KAHAN>(acc[k], cmp[k], val);
+          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) sum[k] += val;
           u += du;
           v += dv;
         }
@@ -263,12 +266,16 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
           const float2 t0 = e[0], t1 = e[fw];
           const float f = one_plus_frac23(u);
           const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          acc_add<KAHAN>(acc[k], cmp[k], fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0));
+          sum[k] += fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
           u += du;
           v += dv;
         }
       }
     }
+  }
+  if (KAHAN) {
+#pragma unroll
+    for (int k = 0; k < kNV; ++k) kahan_add(acc[k], cmp[k], part[k]);
   }
 }
 
@@ -418,18 +425,21 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// One volume tile (bx, by, bz) of a TMA-staged back-projection.  dsm is the
+// CTA's dynamic shared memory laid out by the launcher, mbar its two
+// initialised mbarriers, and uses[b] the completed phases of mbarrier b so far
+// (a persistent CTA runs many tiles on the same mbarriers).  Returns false
+// when a bounded wait ran out (err words set; the tile's voxels untouched).
 template <int MODE, bool SEP, typename IT>
-__global__ void __launch_bounds__(kThreads)
-    bp_tma_kernel(const BpArgs a, const __grid_constant__ CUtensorMap tmap) {
+__device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *tmap, int bx,
+                                            int by, int bz, unsigned char *dsm,
+                                            unsigned long long *mbar, unsigned (&uses)[2]) {
   constexpr bool KAHAN = !std::is_same<IT, float>::value;
-  extern __shared__ __align__(128) unsigned char dsm[];
-  __shared__ __align__(8) unsigned long long mbar[2];
-
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int wy = (tid >> 5) % kTY;
   const int wz = (tid >> 5) / kTY;
-  const int xc = blockIdx.x * kTX, yc = blockIdx.y * kTY, zl = blockIdx.z * kTZ;
+  const int xc = bx * kTX, yc = by * kTY, zl = bz * kTZ;
   const int zc = zl + a.v.zoff;
   const int fw = a.fw, fh = SEP ? kTY : a.fh;
   const int pnx = a.img.nx, pny = a.img.ny;
@@ -452,11 +462,6 @@ __global__ void __launch_bounds__(kThreads)
       tt[i].jmin = y0;
     }
   }
-  if (tid == 0) {
-    mbar_init(&mbar[0], 1);
-    mbar_init(&mbar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
   __syncthreads();
 
   const int nchunks = (nt + chunk - 1) / chunk;
@@ -466,7 +471,7 @@ __global__ void __launch_bounds__(kThreads)
     mbar_expect_tx(&mbar[buf], (unsigned)(nc * bw * bh * (int)sizeof(IT)));
     IT *dst = raw0 + (size_t)buf * chunk * rs;
     for (int i = 0; i < nc; ++i)
-      tma_load_3d(dst + (size_t)i * rs, &tmap, tt[c0 + i].kmin & ~(kXAlign - 1),
+      tma_load_3d(dst + (size_t)i * rs, tmap, tt[c0 + i].kmin & ~(kXAlign - 1),
                   tt[c0 + i].jmin, a.t0 + c0 + i, &mbar[buf]);
   };
   if (tid == 0) {
@@ -483,7 +488,8 @@ __global__ void __launch_bounds__(kThreads)
     // ~1 s budget for a copy; a CTA that gives up raises the launch-wide
     // abort word (err[0]) and the sticky report word (err[1]) so that the
     // other CTAs stop waiting too.
-    const bool ok = mbar_wait_bounded(&mbar[buf], (unsigned)((c >> 1) & 1), 1ll << 31, a.err);
+    const unsigned par = (uses[buf] + (unsigned)(c >> 1)) & 1u;
+    const bool ok = mbar_wait_bounded(&mbar[buf], par, 1ll << 31, a.err);
     if (__syncthreads_or(!ok)) {
       // Report, give the copies this CTA still has in flight a bounded
       // chance to land, and leave the volume untouched.
@@ -491,10 +497,11 @@ __global__ void __launch_bounds__(kThreads)
         atomicExch(a.err, 1);
         atomicExch(a.err + 1, 1);
       }
-      mbar_wait_bounded(&mbar[buf], (unsigned)((c >> 1) & 1), 1ll << 28, nullptr);
+      mbar_wait_bounded(&mbar[buf], par, 1ll << 28, nullptr);
       if (c + 1 < nchunks)
-        mbar_wait_bounded(&mbar[buf ^ 1], (unsigned)(((c + 1) >> 1) & 1), 1ll << 28, nullptr);
-      return;
+        mbar_wait_bounded(&mbar[buf ^ 1], (uses[buf ^ 1] + (unsigned)((c + 1) >> 1)) & 1u,
+                          1ll << 28, nullptr);
+      return false;
     }
     const IT *R0 = raw0 + (size_t)buf * chunk * rs;
     EntryWalk w(tid, fh, fw);
@@ -549,7 +556,29 @@ __global__ void __launch_bounds__(kThreads)
                                     pny, lane, wy, wz);
     __syncthreads();
   }
+  uses[0] += (unsigned)(nchunks + 1) / 2;
+  uses[1] += (unsigned)nchunks / 2;
   bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
+  return true;
+}
+
+__device__ __forceinline__ void mbar_init_pair(unsigned long long *mbar) {
+  if (threadIdx.x == 0) {
+    mbar_init(&mbar[0], 1);
+    mbar_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+template <int MODE, bool SEP, typename IT>
+__global__ void __launch_bounds__(kThreads, 4)
+    bp_tma_kernel(const BpArgs a, const __grid_constant__ CUtensorMap tmap) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+  mbar_init_pair(mbar);
+  unsigned uses[2] = {0u, 0u};
+  bp_tma_tile<MODE, SEP, IT>(a, &tmap, blockIdx.x, blockIdx.y, blockIdx.z, dsm, mbar, uses);
 }
 
 // Forward projection: voxel splat (Reproject, main/main-mpi.cpp:286-344) of
@@ -576,8 +605,8 @@ __global__ void __launch_bounds__(kThreads)
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
 template <bool SEP>
-__global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
-  extern __shared__ float accs[];
+__device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
+                                        float *accs) {
   __shared__ TileTilt tt[kMaxChunk];
   __shared__ SepW sw[kMaxChunk][kTY];
 
@@ -585,7 +614,7 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
   const int lane = tid & 31;
   const int wy = (tid >> 5) % kTY;
   const int wz = (tid >> 5) / kTY;
-  const int xc = blockIdx.x * kFX, yc = blockIdx.y * kTY, zl = blockIdx.z * kFTZ;
+  const int xc = bx * kFX, yc = by * kTY, zl = bz * kFTZ;
   const int zc = zl + a.v.zoff;
   const int fw = a.fw, fh = SEP ? kTY : a.fh;
   const int per = fh * fw;
@@ -739,6 +768,12 @@ __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
   }
 }
 
+template <bool SEP>
+__global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
+  extern __shared__ float accs[];
+  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs);
+}
+
 // SIRT residual (main/main-mpi.cpp:640-647): r = p - (wt != 0 ? val/wt : val),
 // written over val.
 __global__ void resid_kernel(const float *__restrict__ p, float *val,
@@ -834,6 +869,183 @@ __global__ void resid_lp_kernel(const PT *__restrict__ p, const float *__restric
   }
 }
 
+// ---------------------------------------------------------------- batches
+//
+// One batch step: zero the accumulators of the step's forward projections
+// (and reset the work counters), forward-project every item, form every
+// residual, back-project every item.  The forward and back-projection kernels
+// are persistent: each CTA takes the next tile of any item from the table's
+// counter until all are done, so small and large tilt series share the waves.
+
+template <typename Item>
+__device__ __forceinline__ int find_item(const Item *items, int n, long long t) {
+  int lo = 0, hi = n - 1;  // last item whose first tile <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].first <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void zero_batch_kernel(BatchTable *T) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    T->h.bp_next = 0ull;
+    T->h.fp_next = 0ull;
+    if (T->h.err) T->h.err[0] = 0;
+  }
+  const int n = T->h.nzero;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int j = 0; j < n; ++j) {
+    float *p = T->zero[j].p;
+    const size_t cnt = T->zero[j].n;
+    const size_t n4 = (reinterpret_cast<uintptr_t>(p) & 15) ? 0 : cnt / 4;
+    float4 *p4 = reinterpret_cast<float4 *>(p);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += stride)
+      p4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (size_t i = 4 * n4 + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += stride)
+      p[i] = 0.f;
+  }
+}
+
+__device__ __forceinline__ float load_elem(const void *p, int dtype, size_t i) {
+  if (dtype == IMG_F16) return __half2float(reinterpret_cast<const __half *>(p)[i]);
+  if (dtype == IMG_BF16) return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(p)[i]);
+  return reinterpret_cast<const float *>(p)[i];
+}
+
+__device__ __forceinline__ void store_elem(void *p, int dtype, size_t i, float v) {
+  if (dtype == IMG_F16) reinterpret_cast<__half *>(p)[i] = __float2half_rn(v);
+  else if (dtype == IMG_BF16) reinterpret_cast<__nv_bfloat16 *>(p)[i] = __float2bfloat16_rn(v);
+  else reinterpret_cast<float *>(p)[i] = v;
+}
+
+__global__ void resid_batch_kernel(const BatchTable *T) {
+  const int n = T->h.nres;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int j = 0; j < n; ++j) {
+    const BatchRes &R = T->res[j];
+    for (int t = 0; t < R.nt; ++t) {
+      const float sp = R.ps ? R.ps[t] : 1.f;
+      const float inv = R.rs ? 1.f / R.rs[t] : 1.f;  // exact: powers of two
+      const size_t off = R.plane * t;
+      for (size_t i = off + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < off + R.plane;
+           i += stride) {
+        float v = R.val[i];
+        const float w = R.wt[i];
+        if (w != 0.f) v /= w;
+        store_elem(R.r, R.rdtype, i, (load_elem(R.p, R.pdtype, i) * sp - v) * inv);
+      }
+    }
+  }
+}
+
+// FP16 residual items: per-tilt maxima of the FP32 residual, then the
+// conversion with power-of-two scales (as tr_quantize).
+__global__ void absmax_batch_kernel(const BatchTable *T) {
+  const int n = T->h.nres;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int j = 0; j < n; ++j) {
+    const BatchRes &R = T->res[j];
+    if (!R.q) continue;
+    const float *v = reinterpret_cast<const float *>(R.r);
+    for (int t = 0; t < R.nt; ++t) {
+      const size_t off = R.plane * t;
+      float m = 0.f;
+      for (size_t i = off + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < off + R.plane;
+           i += stride) {
+        const float a = fabsf(v[i]);
+        m = a > m ? a : m;
+      }
+      for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(R.qmax + t, __float_as_uint(m));
+    }
+  }
+}
+
+__global__ void quantize_batch_kernel(const BatchTable *T) {
+  const int n = T->h.nres;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int j = 0; j < n; ++j) {
+    const BatchRes &R = T->res[j];
+    if (!R.q) continue;
+    const float *v = reinterpret_cast<const float *>(R.r);
+    for (int t = 0; t < R.nt; ++t) {
+      const int e = scale_exp<__half>(R.qmax[t]);
+      if (blockIdx.x == 0 && threadIdx.x == 0) R.qscale[t] = pow2f(e);
+      const float inv = pow2f(-e);
+      const size_t off = R.plane * t;
+      for (size_t i = off + blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < off + R.plane;
+           i += stride)
+        R.q[i] = __float2half_rn(v[i] * inv);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
+  extern __shared__ float accs[];
+  __shared__ long long s_tile;
+  __shared__ int s_item;
+  const long long total = T->h.fp_tiles;
+  const int n = T->h.nfp;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long t = (long long)atomicAdd(&T->h.fp_next, 1ull);
+      s_tile = t;
+      s_item = t < total ? find_item(T->fp, n, t) : -1;
+    }
+    __syncthreads();
+    const long long t = s_tile;
+    if (t >= total) break;
+    const BatchFp &it = T->fp[s_item];
+    long long l = t - it.first;
+    const int bx = (int)(l % it.gx);
+    l /= it.gx;
+    const int by = (int)(l % it.gy), bz = (int)(l / it.gy);
+    if (it.sep) fp_tile<true>(it.a, bx, by, bz, accs);
+    else fp_tile<false>(it.a, bx, by, bz, accs);
+  }
+}
+
+// Back-projection items: BP_NORM over FP32 images (filtered projections) and
+// BP_SIRT over residuals of type RT.
+template <typename RT>
+__global__ void __launch_bounds__(kThreads, 4) bp_batch_kernel(BatchTable *T) {
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ __align__(8) unsigned long long mbar[2];
+  __shared__ long long s_tile;
+  __shared__ int s_item;
+  mbar_init_pair(mbar);
+  unsigned uses[2] = {0u, 0u};
+  const long long total = T->h.bp_tiles;
+  const int n = T->h.nbp;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const long long t = (long long)atomicAdd(&T->h.bp_next, 1ull);
+      s_tile = t;
+      s_item = t < total ? find_item(T->bp, n, t) : -1;
+    }
+    __syncthreads();
+    const long long t = s_tile;
+    if (t >= total) break;
+    const BatchBp &it = T->bp[s_item];
+    long long l = t - it.first;
+    const int bx = (int)(l % it.gx);
+    l /= it.gx;
+    const int by = (int)(l % it.gy), bz = (int)(l / it.gy);
+    bool ok;
+    if (it.mode == BP_NORM)
+      ok = it.sep ? bp_tma_tile<BP_NORM, true, float>(it.a, &it.map, bx, by, bz, dsm, mbar, uses)
+                  : bp_tma_tile<BP_NORM, false, float>(it.a, &it.map, bx, by, bz, dsm, mbar, uses);
+    else
+      ok = it.sep ? bp_tma_tile<BP_SIRT, true, RT>(it.a, &it.map, bx, by, bz, dsm, mbar, uses)
+                  : bp_tma_tile<BP_SIRT, false, RT>(it.a, &it.map, bx, by, bz, dsm, mbar, uses);
+    if (!ok) break;
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 
 static dim3 tile_grid(const VolView &v) {
@@ -883,44 +1095,57 @@ constexpr CUtensorMapDataType tma_type() {
                                            : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
 }
 
-template <int MODE, bool SEP, typename IT>
-static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err) {
+// TMA staging layout of a back-projection within `budget` bytes of dynamic
+// shared memory: tile bookkeeping, two raw window buffers per staged tilt and
+// the interpolation tables.  Fills the tensor map, the chunk and the tma_*
+// fields; false when the images or the window do not suit TMA.
+template <typename IT>
+static bool tma_layout(const BpArgs &a0, bool sep, size_t budget, BpArgs *out,
+                       CUtensorMap *map, size_t *smem) {
   const ImgView &im = a0.img;
   constexpr int es = (int)sizeof(IT);
   constexpr int xal = 16 / es;  // TMA x coordinates and box widths: 16-byte multiples
   if (!im.p || !a0.err || (im.nx * es) % 16 != 0 ||
       (reinterpret_cast<uintptr_t>(im.p) & 15) != 0)
     return false;
-  const int fh = SEP ? kTY : a0.fh;
+  const int fh = sep ? kTY : a0.fh;
   const int bw = (a0.fw + xal + xal - 1) / xal * xal;
-  const int bh = SEP ? kTY + 3 : fh + 1;
+  const int bh = sep ? kTY + 3 : fh + 1;
   if (bw > 256 || bh > 256) return false;
   const int rs = ((bw * bh * es + 127) & ~127) / es;  // elements; 128-byte aligned slots
   const size_t fixed =
       ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
   const size_t per_tilt = 2 * (size_t)rs * es + (size_t)fh * a0.fw * sizeof(float2);
-  if (fixed + per_tilt > kSmemTma + 64 * 1024) return false;
-  int chunk = (int)std::max<size_t>(1, (kSmemTma > fixed ? kSmemTma - fixed : 0) / per_tilt);
+  if (fixed + per_tilt > budget + 64 * 1024) return false;
+  int chunk = (int)std::max<size_t>(1, (budget > fixed ? budget - fixed : 0) / per_tilt);
   chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
-  const size_t smem = fixed + (size_t)chunk * per_tilt;
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) return false;
-  CUtensorMap map;
   const cuuint64_t dims[3] = {(cuuint64_t)im.nx, (cuuint64_t)im.ny,
                               (cuuint64_t)(a0.t0 + a0.nt)};
   const cuuint64_t strides[2] = {(cuuint64_t)im.nx * es, (cuuint64_t)im.tstride * es};
   const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  if (enc(&map, tma_type<IT>(), 3, const_cast<float *>(im.p), dims, strides, box, estr,
+  if (enc(map, tma_type<IT>(), 3, const_cast<float *>(im.p), dims, strides, box, estr,
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  BpArgs a = a0;
-  a.chunk = chunk;
-  a.tma_bw = bw;
-  a.tma_bh = bh;
-  a.tma_raw_stride = rs;
-  a.tma_raw_offset = (int)fixed;
+  *out = a0;
+  out->chunk = chunk;
+  out->tma_bw = bw;
+  out->tma_bh = bh;
+  out->tma_raw_stride = rs;
+  out->tma_raw_offset = (int)fixed;
+  *smem = fixed + (size_t)chunk * per_tilt;
+  return true;
+}
+
+template <int MODE, bool SEP, typename IT>
+static bool try_launch_bp_tma(const BpArgs &a0, cudaStream_t s, cudaError_t *err) {
+  BpArgs a;
+  CUtensorMap map;
+  size_t smem = 0;
+  if (!tma_layout<IT>(a0, SEP, kSmemTma, &a, &map, &smem)) return false;
   cudaError_t e = cudaFuncSetAttribute(bp_tma_kernel<MODE, SEP, IT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
@@ -1033,6 +1258,69 @@ cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const fl
     resid_lp_rt((const __nv_bfloat16 *)p, ps, val, wt, plane, nt, rdtype, r, rs, nsm, s);
   else
     resid_lp_rt((const float *)p, ps, val, wt, plane, nt, rdtype, r, rs, nsm, s);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------- batch host helpers
+
+dim3 bp_tile_grid(const VolView &v) { return tile_grid(v); }
+dim3 fp_tile_grid(const VolView &v) { return fp_grid(v); }
+
+// TMA layout of one back-projection item within `budget` bytes of shared
+// memory (image element type by a.img.dtype); false when unsuitable.
+bool batch_bp_layout(const BpArgs &a0, bool sep, size_t budget, BatchBp *out, size_t *smem) {
+  BpArgs a;
+  bool ok;
+  if (a0.img.dtype == IMG_F16) ok = tma_layout<__half>(a0, sep, budget, &a, &out->map, smem);
+  else if (a0.img.dtype == IMG_BF16)
+    ok = tma_layout<__nv_bfloat16>(a0, sep, budget, &a, &out->map, smem);
+  else ok = tma_layout<float>(a0, sep, budget, &a, &out->map, smem);
+  if (ok) out->a = a;
+  return ok;
+}
+
+template <typename RT>
+static cudaError_t set_bp_batch_smem(size_t smem) {
+  return cudaFuncSetAttribute(bp_batch_kernel<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)smem);
+}
+
+// Resident CTAs per SM of the persistent kernels at the given shared memory.
+int batch_occupancy(int rdtype, size_t smem_bp, size_t smem_fp, int *fp_per_sm) {
+  int nb = 0, nf = 0;
+  cudaFuncSetAttribute(fp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem_fp);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nf, fp_batch_kernel, kThreads, smem_fp);
+  if (rdtype == IMG_F16) {
+    set_bp_batch_smem<__half>(smem_bp);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bp_batch_kernel<__half>, kThreads, smem_bp);
+  } else if (rdtype == IMG_BF16) {
+    set_bp_batch_smem<__nv_bfloat16>(smem_bp);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bp_batch_kernel<__nv_bfloat16>, kThreads,
+                                                  smem_bp);
+  } else {
+    set_bp_batch_smem<float>(smem_bp);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, bp_batch_kernel<float>, kThreads, smem_bp);
+  }
+  *fp_per_sm = nf;
+  return nb;
+}
+
+// The six launches of one step over the table at T (device).  The kernels'
+// shared-memory limits are set beforehand by batch_occupancy.
+cudaError_t launch_batch_step(BatchTable *T, int rdtype, int grid_fp, int grid_bp,
+                              size_t smem_fp, size_t smem_bp, int nsm, cudaStream_t s) {
+  zero_batch_kernel<<<nsm * 4, 256, 0, s>>>(T);
+  fp_batch_kernel<<<grid_fp, kThreads, smem_fp, s>>>(T);
+  resid_batch_kernel<<<nsm * 4, 256, 0, s>>>(T);
+  absmax_batch_kernel<<<nsm * 4, 256, 0, s>>>(T);
+  quantize_batch_kernel<<<nsm * 4, 256, 0, s>>>(T);
+  if (rdtype == IMG_F16)
+    bp_batch_kernel<__half><<<grid_bp, kThreads, smem_bp, s>>>(T);
+  else if (rdtype == IMG_BF16)
+    bp_batch_kernel<__nv_bfloat16><<<grid_bp, kThreads, smem_bp, s>>>(T);
+  else
+    bp_batch_kernel<float><<<grid_bp, kThreads, smem_bp, s>>>(T);
   return cudaGetLastError();
 }
 

@@ -26,14 +26,9 @@
 #include <mutex>
 
 #include "tiltrec_b200.h"
+#include "tr_geom.h"
 #include "tr_internal.cuh"
 
-namespace trb {
-cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
-cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
-cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n,
-                         int nsm, cudaStream_t s);
-}  // namespace trb
 
 using namespace trb;
 
@@ -81,56 +76,18 @@ struct StaticGeom {
 // kernels stage.
 bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
             StaticGeom *out) {
-  bool sep = true;
-  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
-  const double two32 = 4294967296.0;
-  const double ext = std::max(std::max(nx, ny), th) + 64.0;
-  for (int t = 0; t < nt; ++t) {
-    const double *k = coeff8 + 8 * (size_t)t;
-    for (int i = 0; i < 4; ++i) {
-      if (!std::isfinite(k[i]) || !std::isfinite(k[4 + i])) return false;
-      g[t].a[i] = k[i];
-      g[t].b[i] = k[4 + i];
-    }
-    for (int i = 0; i < 3; ++i) {
-      if (fabs(k[1 + i]) > 1024.0 || fabs(k[5 + i]) > 1024.0) return false;
-      g[t].A[i] = llrint(k[1 + i] * two32);
-      g[t].B[i] = llrint(k[5 + i] * two32);
-    }
-    if (fabs(k[0]) + (fabs(k[1]) + fabs(k[2]) + fabs(k[3])) * 2 * ext > 1.0e9 ||
-        fabs(k[4]) + (fabs(k[5]) + fabs(k[6]) + fabs(k[7])) * 2 * ext > 1.0e9)
-      return false;
-    if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
-    min_a1 = std::min(min_a1, fabs(k[1]));
-    span_u = std::max(span_u, fabs(k[1]) * (kTX - 1) + fabs(k[2]) * (kTY - 1) +
-                                  fabs(k[3]) * (kTZ - 1));
-    span_v = std::max(span_v, fabs(k[5]) * (kTX - 1) + fabs(k[6]) * (kTY - 1) +
-                                  fabs(k[7]) * (kTZ - 1));
-    fspan_u = std::max(fspan_u, fabs(k[1]) * (kFX - 1) + fabs(k[2]) * (kTY - 1) +
-                                    fabs(k[3]) * (kFTZ - 1));
-    fspan_v = std::max(fspan_v, fabs(k[5]) * (kFX - 1) + fabs(k[6]) * (kTY - 1) +
-                                    fabs(k[7]) * (kFTZ - 1));
-  }
-  out->fw = (int)ceil(span_u) + 4;
-  out->fh = sep ? kTY : (int)ceil(span_v) + 5;
-  out->ffw = (int)ceil(fspan_u) + 4;
-  out->ffh = sep ? kTY : (int)ceil(fspan_v) + 5;
-  out->sep = sep;
-  {
-    // forward-projection window bound, as the context path computes it
-    double bx = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
-    bx = std::min(bx, (double)kFX);
-    out->nbound = (float)(bx * kTY * kFTZ);
-  }
-  const size_t ent_bp = (size_t)out->fw * out->fh * sizeof(float2);
-  const size_t ent_fp = (size_t)out->ffw * out->ffh * sizeof(float);
-  if (ent_bp > kStaticSmemMax || ent_fp > kStaticSmemMax) return false;
-  if (std::max(std::max(out->fw, out->fh), std::max(out->ffw, out->ffh)) > kMaxWindow)
+  GeomInfo gi;
+  int bad = -1;
+  if (derive_geometry(coeff8, nt, nx, ny, th, kStaticSmemMax, g, &gi, &bad) != GEOM_OK)
     return false;
-  out->chunk_bp =
-      (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemBp / ent_bp));
-  out->chunk_fp =
-      (int)std::max<size_t>(1, std::min<size_t>(kMaxChunk, kStaticSmemFp / ent_fp));
+  out->fw = gi.fw;
+  out->fh = gi.fh;
+  out->ffw = gi.ffw;
+  out->ffh = gi.ffh;
+  out->sep = gi.sep;
+  out->nbound = gi.nbound;
+  out->chunk_bp = chunk_for(kStaticSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
+  out->chunk_fp = chunk_for(kStaticSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
   return true;
 }
 

@@ -184,3 +184,26 @@ def project_series(engine, cfg: Config, layout: int = 0, noise: str = "gaussian"
         raise ValueError(noise)
     torch.cuda.synchronize()
     return proj.contiguous()
+
+
+def batch_series(n: int = 64, seed: int = 3) -> list[Config]:
+    """The batched configuration's tilt series (seeded): projection size
+    drawn from {512^2, 1024^2, 2048^2}, tilt count from {41, 61, 81} over
+    +-U(60, 70) degrees, thickness U(64, 384) voxels; cfg0's ellipsoid and
+    bead phantom (50 + 20 objects, per-tilt offsets N(0, 1 px), noise 0.1 std)
+    with lengths scaled to the projection size.  Each series is WBP followed
+    by SIRT-10 (relaxation 0.5) from the WBP result."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        size = int(rng.choice([512, 1024, 2048]))
+        nt = int(rng.choice([41, 61, 81]))
+        amax = float(rng.uniform(60.0, 70.0))
+        th = int(rng.uniform(64, 384))
+        c = Config(f"batch{i}", size, size, th,
+                   np.linspace(-amax, amax, nt).astype(np.float32), 50, 20,
+                   seed * 1000 + i, offset_sigma=1.0, noise=0.1, method="WBP+SIRT",
+                   iters=10, gamma=0.5)
+        c.extra["scale"] = 256.0 / size
+        out.append(c)
+    return out

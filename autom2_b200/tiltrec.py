@@ -315,3 +315,118 @@ def static_scratch_limit() -> int:
     lib = load_library()
     lib.tr_static_scratch_limit.restype = C.c_size_t
     return int(lib.tr_static_scratch_limit())
+
+
+# ------------------------------------------------------------ batched jobs
+
+class Job(C.Structure):
+    """tr_job: one reconstruction for the scheduler."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("ntilt", C.c_int), ("thickness", C.c_int),
+                ("layout", C.c_int), ("coeff8", C.POINTER(C.c_double)),
+                ("ox", C.c_float), ("oy", C.c_float), ("oz", C.c_float),
+                ("proj", C.c_void_p), ("vol", C.c_void_p), ("vol_in", C.c_int),
+                ("host", C.c_int),
+                ("wbp", C.c_int), ("sirt_iters", C.c_int), ("gamma", C.c_float)]
+
+
+class SchedInfo(C.Structure):
+    _fields_ = [("steps", C.c_longlong), ("bp_items", C.c_longlong),
+                ("fp_items", C.c_longlong), ("peak_bytes", C.c_size_t),
+                ("grid_bp", C.c_int), ("grid_fp", C.c_int), ("smem_bp", C.c_size_t),
+                ("queued", C.c_int), ("active", C.c_int)]
+
+
+class Scheduler:
+    """tr_sched: many reconstructions on one device, advanced together one
+    batched step at a time (see include/tiltrec_b200.h).
+
+    Jobs take torch CUDA tensors (device jobs: the volume is updated in
+    place) or numpy arrays (host jobs: pinned memory overlaps the copies)."""
+
+    def __init__(self, device=0, hbm_budget=0, proj_dtype="f32", resid_dtype="f32"):
+        self.lib = load_library()
+        L = self.lib
+        vp, i, sz = C.c_void_p, C.c_int, C.c_size_t
+        L.tr_sched_create.argtypes = [i, sz, i, i, C.POINTER(vp)]
+        L.tr_sched_submit.argtypes = [vp, C.POINTER(Job), C.POINTER(C.c_ulonglong)]
+        L.tr_sched_wait.argtypes = [vp, C.c_ulonglong, C.POINTER(C.c_double)]
+        L.tr_sched_drain.argtypes = [vp]
+        L.tr_sched_stats.argtypes = [vp, C.POINTER(SchedInfo)]
+        L.tr_sched_last_error.argtypes = [vp]
+        L.tr_sched_last_error.restype = C.c_char_p
+        L.tr_sched_configure.argtypes = [vp, sz, i]
+        L.tr_sched_autotune.argtypes = [vp, C.POINTER(Job), i, C.POINTER(sz), C.POINTER(i)]
+        L.tr_sched_destroy.argtypes = [vp]
+        h = vp()
+        st = L.tr_sched_create(device, hbm_budget, DTYPES[proj_dtype], DTYPES[resid_dtype],
+                               C.byref(h))
+        if st:
+            raise TiltRecError(st, "tr_sched_create failed")
+        self.h = h
+        self.device = device
+
+    def _check(self, st, what):
+        if st:
+            raise TiltRecError(st, f"{what}: {self.lib.tr_sched_last_error(self.h).decode()}")
+
+    def job(self, proj, vol, coeff8, layout=LAYOUT_Y, origin=None, wbp=False, sirt_iters=0,
+            gamma=0.0, vol_in=False):
+        """A tr_job over proj [nt][ny][nx] and vol (the layout's shape); the
+        reconstruction starts from vol's contents when vol_in, else from
+        zeros."""
+        nt, ny, nx = proj.shape
+        th = vol.shape[1] if layout == LAYOUT_Y else vol.shape[0]
+        c = np.ascontiguousarray(coeff8, np.float64).reshape(nt, 8)
+        ox, oy, oz = origin if origin is not None else default_origin(layout, nx, ny, th)
+        host = isinstance(proj, np.ndarray)
+        if host:
+            assert proj.dtype == np.float32 and vol.dtype == np.float32
+            assert proj.flags.c_contiguous and vol.flags.c_contiguous
+            pp, vv = proj.ctypes.data, vol.ctypes.data
+        else:
+            pp, vv = proj.data_ptr(), vol.data_ptr()
+        j = Job(nx, ny, nt, th, layout, c.ctypes.data_as(C.POINTER(C.c_double)), ox, oy, oz,
+                pp, vv, int(bool(vol_in)), int(host), int(bool(wbp)), sirt_iters, gamma)
+        j._c = c  # keeps the coefficients alive until submission copies them
+        return j
+
+    def submit(self, job: Job) -> int:
+        jid = C.c_ulonglong()
+        self._check(self.lib.tr_sched_submit(self.h, C.byref(job), C.byref(jid)),
+                    "tr_sched_submit")
+        return jid.value
+
+    def wait(self, jid: int) -> float:
+        """Blocks until job jid is done; returns its latency in seconds."""
+        lat = C.c_double()
+        self._check(self.lib.tr_sched_wait(self.h, jid, C.byref(lat)), "tr_sched_wait")
+        return lat.value
+
+    def drain(self):
+        self._check(self.lib.tr_sched_drain(self.h), "tr_sched_drain")
+
+    def stats(self) -> dict:
+        info = SchedInfo()
+        self._check(self.lib.tr_sched_stats(self.h, C.byref(info)), "tr_sched_stats")
+        return {k: getattr(info, k) for k, _ in SchedInfo._fields_}
+
+    def configure(self, smem_bp: int, bp_ctas_per_sm: int = 0):
+        self._check(self.lib.tr_sched_configure(self.h, smem_bp, bp_ctas_per_sm),
+                    "tr_sched_configure")
+
+    def autotune(self, probe: Job, iters: int = 2):
+        sm, ct = C.c_size_t(), C.c_int()
+        self._check(self.lib.tr_sched_autotune(self.h, C.byref(probe), iters, C.byref(sm),
+                                               C.byref(ct)), "tr_sched_autotune")
+        return sm.value, ct.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tr_sched_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

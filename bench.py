@@ -415,6 +415,240 @@ def run_kernels(args):
     eng.close()
 
 
+class OutputPool:
+    """Reusable output volumes per projection size (the batch and serving
+    runs keep only this many results alive at once)."""
+
+    def __init__(self, make, sizes_counts):
+        import threading as th
+        self.cv = th.Condition()
+        self.free = {k: [make(k) for _ in range(n)] for k, n in sizes_counts.items()}
+
+    def take(self, key):
+        with self.cv:
+            self.cv.wait_for(lambda: bool(self.free[key]))
+            return self.free[key].pop()
+
+    def give(self, key, buf):
+        with self.cv:
+            self.free[key].append(buf)
+            self.cv.notify_all()
+
+
+def job_vpu(c, wbp, iters):
+    """Voxel-projection updates of one job: WBP one pass, SIRT two per
+    iteration."""
+    return (int(wbp) + 2 * iters) * c.ntilt * c.nx * c.ny * c.thickness
+
+
+def run_batch(args):
+    """Batched configuration: 64 uneven tilt series, WBP then SIRT-10 each,
+    run (1) one at a time through the engine in FP32 (the plain GPU form) and
+    (2) all together through the scheduler (persistent graph-replayed steps,
+    16-bit storage).  Inputs are device-resident; one JSON line."""
+    import torch
+
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+    build.build_lib()
+    torch.cuda.set_device(0)
+    specs = synth.batch_series(args.jobs or 64, seed=3)
+    eng = T.Engine(0)
+    series = []
+    for c in specs:
+        c8 = synth.coefficients(c)
+        eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
+        series.append((c, c8, synth.project_series(eng, c, 0, "gaussian")))
+    total_vpu = sum(job_vpu(c, True, c.iters) for c, _, _ in series)
+    cmp_idx = [i for i, (c, _, _) in enumerate(series) if c.nx <= 1024][:4]
+
+    def vol_for(buf, c):
+        return buf[: c.ny * c.thickness * c.nx].view(c.ny, c.thickness, c.nx)
+
+    # (1) plain FP32, one series at a time
+    maxv = max(c.nx * c.ny * c.thickness for c, _, _ in series)
+    buf = torch.empty(maxv, device="cuda")
+    plain_ref = {}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, (c, c8, proj) in enumerate(series):
+        eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
+        v = vol_for(buf, c)
+        v.zero_()
+        f = proj.clone()
+        eng.wbp(f, v)
+        del f
+        eng.sirt(proj, v, c.iters, c.gamma)
+        if i in cmp_idx:
+            plain_ref[i] = v.clone()
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    del buf
+    eng.close()
+
+    # (2) the scheduler, all jobs submitted at once
+    counts = {512: 8, 1024: 6, 2048: 4}
+    pool = OutputPool(lambda n: torch.empty(n * n * 384, device="cuda"), counts)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free - 8e9)
+    S = T.Scheduler(0, hbm_budget=budget, proj_dtype=args.storage, resid_dtype=args.storage)
+    probe_i = next(i for i, (c, _, _) in enumerate(series) if c.nx == 1024)
+    c, c8, proj = series[probe_i]
+    pv = torch.zeros((c.ny, c.thickness, c.nx), device="cuda")
+    tuned = S.autotune(S.job(proj, pv, c8, T.LAYOUT_Y, sirt_iters=2, gamma=c.gamma))
+    del pv
+    results = {}
+    lat = [0.0] * len(series)
+    errs = []
+    import threading as th
+
+    def waiter(i, jid, key, b):
+        lat[i] = S.wait(jid)
+        if i in cmp_idx:
+            results[i] = vol_for(b, series[i][0]).clone()
+        pool.give(key, b)
+
+    threads = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i, (c, c8, proj) in enumerate(series):
+        b = pool.take(c.nx)
+        v = vol_for(b, c)
+        jid = S.submit(S.job(proj, v, c8, T.LAYOUT_Y, wbp=True, sirt_iters=c.iters,
+                             gamma=c.gamma))
+        t = th.Thread(target=waiter, args=(i, jid, c.nx, b))
+        t.start()
+        threads.append(t)
+    for t in threads:
+        t.join()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    info = S.stats()
+    S.close()
+    for i in cmp_idx:
+        a, r = results[i].double(), plain_ref[i].double()
+        errs.append(float((a - r).norm() / r.norm()))
+    line = {"workload": "batch", "metric": "voxel-proj updates/s", "unit": "VPU/s",
+            "value": total_vpu / t_batch, "n_gpus": 1, "higher_is_better": True,
+            "jobs": len(series), "recon_per_hour": len(series) / t_batch * 3600,
+            "seconds": t_batch, "dtype": f"{args.storage} storage, f32 accumulate",
+            "plain": {"value": total_vpu / t_plain, "seconds": t_plain,
+                      "recon_per_hour": len(series) / t_plain * 3600, "dtype": "f32",
+                      "form": "one series at a time, engine tr_wbp + tr_sirt"},
+            "speedup_vs_plain": t_plain / t_batch,
+            "rel_l2_vs_plain_f32": {"max": max(errs), "jobs": cmp_idx},
+            "p50_latency_s": statistics.median(lat), "autotune": {"smem_bp": tuned[0],
+                                                                   "ctas_per_sm": tuned[1]},
+            "scheduler": info, "data": "synthetic",
+            "config": {"series": "64 seeded: N in {512,1024,2048}, T in {41,61,81} over "
+                                 "+-U(60,70) deg, th U(64,384); WBP then SIRT-10 (0.5)",
+                       "budget_bytes": budget}}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Serving configuration: Poisson arrivals of jobs drawn from the batched
+    configuration's series (host buffers in, host volume out), methods uniform
+    over WBP, SIRT-10, SIRT-30.  The scheduler (continuous batching under the
+    HBM budget, 16-bit storage) and the plain GPU form (one job at a time
+    through tr_reconstruct_host, FP32, FIFO) see the same arrival times; both
+    report p50/p99 latency from arrival to the volume in host memory."""
+    import threading as th
+
+    import torch
+
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+    build.build_lib()
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(7)
+    pool_specs = synth.batch_series(args.series, seed=7)
+    eng = T.Engine(0)
+    series = []
+    for c in pool_specs:
+        c8 = synth.coefficients(c)
+        eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
+        p = synth.project_series(eng, c, 0, "gaussian").cpu().pin_memory()
+        out = torch.zeros((c.ny, c.thickness, c.nx)).pin_memory()
+        series.append((c, c8, p.numpy(), out.numpy(), p, out))
+    methods = [("WBP", True, 0), ("SIRT-10", False, 10), ("SIRT-30", False, 30)]
+    njobs = args.jobs or 64
+    jobs = [(int(rng.integers(len(series))), methods[int(rng.integers(3))]) for _ in range(njobs)]
+    mean_vpu = float(np.mean([job_vpu(series[s][0], m[1], m[2]) for s, m in jobs]))
+    rate = args.rate
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, njobs))
+    busy = [th.Lock() for _ in series]  # one output buffer per series
+
+    def run_form(submit_fn):
+        lat = [0.0] * njobs
+        done_at = [0.0] * njobs
+        threads = []
+        t0 = time.perf_counter()
+
+        def one(k):
+            s, m = jobs[k]
+            delay = t0 + arrivals[k] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            with busy[s]:
+                submit_fn(s, m)
+                done_at[k] = time.perf_counter()
+            lat[k] = done_at[k] - (t0 + arrivals[k])
+
+        for k in range(njobs):
+            t = th.Thread(target=one, args=(k,))
+            t.start()
+            threads.append(t)
+        for t in threads:
+            t.join()
+        return lat, max(done_at) - t0
+
+    # plain: one job at a time in arrival order (a FIFO single server)
+    fifo = th.Lock()
+
+    def plain_submit(s, m):
+        c, c8, pnp, onp, _, _ = series[s]
+        with fifo:
+            eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
+            onp[...] = 0
+            eng.reconstruct_host("WBP" if m[1] else "SIRT", pnp, onp, m[2], 0.5)
+
+    lat_plain, span_plain = run_form(plain_submit)
+    eng.close()
+    free, _ = torch.cuda.mem_get_info()
+    budget = min(int(args.budget_gb * 1e9), int(free - 8e9))
+    S = T.Scheduler(0, hbm_budget=budget, proj_dtype=args.storage, resid_dtype=args.storage)
+
+    def sched_submit(s, m):
+        c, c8, pnp, onp, _, _ = series[s]
+        S.wait(S.submit(S.job(pnp, onp, c8, T.LAYOUT_Y, wbp=m[1], sirt_iters=m[2],
+                              gamma=0.5)))
+
+    lat_s, span_s = run_form(sched_submit)
+    info = S.stats()
+    S.close()
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q))
+
+    line = {"workload": "serve", "metric": "reconstructions/hour", "unit": "recon/h",
+            "value": njobs / span_s * 3600, "higher_is_better": True, "n_gpus": 1,
+            "jobs": njobs, "arrival_rate_per_s": rate,
+            "offered_vpu_per_s": mean_vpu * rate,
+            "p50_latency_s": pct(lat_s, 50), "p99_latency_s": pct(lat_s, 99),
+            "makespan_s": span_s, "dtype": f"{args.storage} storage, f32 accumulate",
+            "plain": {"value": njobs / span_plain * 3600, "p50_latency_s": pct(lat_plain, 50),
+                      "p99_latency_s": pct(lat_plain, 99), "makespan_s": span_plain,
+                      "form": "FIFO, one job at a time through tr_reconstruct_host, f32"},
+            "speedup_vs_plain": span_plain / span_s, "scheduler": info,
+            "data": "synthetic", "config": {
+                "series_pool": args.series, "methods": "uniform WBP / SIRT-10 / SIRT-30",
+                "host_buffers": "pinned", "budget_bytes": budget,
+                "note": "one output buffer per series: a job waits for it while a job of "
+                        "the same series is in flight (counted in its latency)"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -425,8 +659,20 @@ def main():
                     help="profiling case only (see run_kernels)")
     ap.add_argument("--scale", type=int, default=2)
     ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--workload", default="sirt", choices=["sirt", "batch", "serve"],
+                    help="sirt: the headline SIRT-30 line; batch / serve: the batched "
+                         "and serving configurations (one JSON line each)")
+    ap.add_argument("--jobs", type=int, default=0)
+    ap.add_argument("--series", type=int, default=12)
+    ap.add_argument("--rate", type=float, default=1.0, help="serve: arrivals per second")
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--storage", default="f16", choices=["f32", "f16", "bf16"])
     args = ap.parse_args()
-    if args.kernels:
+    if args.workload == "batch":
+        run_batch(args)
+    elif args.workload == "serve":
+        run_serve(args)
+    elif args.kernels:
         run_kernels(args)
     elif args.impl == "reference":
         run_reference(args)

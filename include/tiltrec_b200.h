@@ -197,13 +197,80 @@ tr_status tr_backproject_lp(tr_ctx *ctx, const void *proj_dev, int dtype,
                             int nz, void *stream);
 
 /* SIRT (as tr_sirt) from a 16-bit stack (proj_dtype, scales from
- * tr_quantize) with the residual stored as resid_dtype (TR_DTYPE_F32, F16 --
- * in the projections' per-tilt scale -- or BF16).  The reprojection,
- * weights and volume stay FP32; the residual back-projection sums are
- * compensated per voxel when the residual is 16-bit. */
+ * tr_quantize; scale_dev may be NULL for TR_DTYPE_F32) with the residual
+ * stored as resid_dtype: TR_DTYPE_F32; F16 with its own per-tilt
+ * power-of-two scales, recomputed every iteration (the residual's range is
+ * not the stack's: after a WBP start it can be far larger); or BF16 (float's
+ * range, no scale).  The reprojection, weights and volume stay FP32; the
+ * residual back-projection sums are compensated per voxel when the residual
+ * is 16-bit. */
 tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
                      const float *scale_dev, int resid_dtype, float *vol_dev,
                      int iters, float gamma, void *stream);
+
+/* ---- Batched jobs and serving.  No counterpart in the reference, which
+ * reconstructs one tilt series per process run.
+ *
+ * A scheduler owns one device and an HBM budget.  Submitted jobs are
+ * admitted in order while their device memory fits the budget; admission
+ * (upload, 16-bit storage of the projections, WBP filtering, weights)
+ * overlaps the running jobs.  All admitted jobs advance together, one step at
+ * a time: a step is one persistent forward-projection launch, one residual
+ * launch and one persistent back-projection launch over the tiles of every
+ * job (a WBP back-projection or one SIRT iteration each), replayed from a
+ * CUDA graph.  A background thread drives the steps; calls are thread-safe.
+ * Results do not depend on the other jobs in the mix beyond the order of the
+ * forward projection's float atomic adds (as for a job run alone).  Images
+ * must suit the TMA staging: rows of a multiple of 16 bytes (nx % 4 == 0 for
+ * FP32 storage, nx % 8 == 0 for 16-bit storage). */
+typedef struct tr_sched tr_sched;
+
+typedef struct {
+  int nx, ny, ntilt, thickness, layout;
+  const double *coeff8;  /* ntilt*8, copied at submission */
+  float ox, oy, oz;      /* origin as for tr_set_problem */
+  const float *proj;     /* FP32 stack [ntilt][ny][nx] */
+  float *vol;            /* result (whole volume); also the starting volume
+                            when vol_in is 1 */
+  int vol_in;            /* 1: start from vol (--initial); 0: start from zeros */
+  int host;              /* 1: proj and vol are host buffers (pinned for overlap);
+                            0: device buffers, vol updated in place */
+  int wbp;               /* 1: add the WBP reconstruction first (--method WBP) */
+  int sirt_iters;        /* then SIRT iterations */
+  float gamma;
+} tr_job;
+
+typedef struct {
+  long long steps, bp_items, fp_items;
+  size_t peak_bytes;     /* most job memory admitted at once */
+  int grid_bp, grid_fp;  /* persistent CTAs of the step launches */
+  size_t smem_bp;        /* back-projection shared-memory budget per CTA */
+  int queued, active;
+} tr_sched_info;
+
+/* proj_dtype: storage of the stack between steps (TR_DTYPE_F32/F16/BF16,
+ * 16-bit with per-tilt power-of-two scales); resid_dtype: SIRT residual
+ * storage (FP16 in the stack's scales). */
+tr_status tr_sched_create(int device, size_t hbm_budget, int proj_dtype,
+                          int resid_dtype, tr_sched **out);
+tr_status tr_sched_submit(tr_sched *s, const tr_job *job, unsigned long long *id);
+/* Blocks until job `id` is done (its volume written); latency from
+ * submission to completion in seconds. */
+tr_status tr_sched_wait(tr_sched *s, unsigned long long id, double *latency_s);
+/* Blocks until every submitted job is done. */
+tr_status tr_sched_drain(tr_sched *s);
+tr_status tr_sched_stats(tr_sched *s, tr_sched_info *out);
+const char *tr_sched_last_error(const tr_sched *s);
+/* Launch configuration of the steps (waits until idle): back-projection
+ * shared-memory budget per CTA and resident CTAs per SM (0: as many as fit). */
+tr_status tr_sched_configure(tr_sched *s, size_t smem_bp, int bp_ctas_per_sm);
+/* Autotuner: times `iters` SIRT steps of a device-resident probe job (run on
+ * a scratch copy of its volume) under candidate configurations -- shared
+ * memory per back-projection CTA (40, 56, 80, 112 KiB) at full residency,
+ * then one resident CTA fewer at the best -- and keeps the fastest. */
+tr_status tr_sched_autotune(tr_sched *s, const tr_job *probe, int iters,
+                            size_t *best_smem_bp, int *best_ctas_per_sm);
+tr_status tr_sched_destroy(tr_sched *s);
 
 /* SIRT that allocates no device memory and needs no context.  No
  * counterpart in the reference.  For callers that cannot call cudaMalloc

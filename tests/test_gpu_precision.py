@@ -147,3 +147,27 @@ def test_sirt_lp_f32_equals_sirt(engine, series):
     engine.sirt(proj, a, 3, 0.5)
     engine.sirt_lp(proj, None, b, 3, 0.5, "f32")
     assert O.rel_l2(host(b), host(a)) < 1e-6
+
+
+def test_sirt_lp_f16_residual_after_wbp(engine, series, restatement):
+    """SIRT from a WBP start (cfg3's WBP-then-SIRT): the residual's range is
+    then far from the stack's, and the FP16 residual must take its own
+    per-tilt scales to stay finite and within the 1e-4 bar."""
+    cfg, c8, org, proj, _, noise = series
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    engine.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Z, org)
+    vol = torch.zeros((th, ny, nx), device="cuda")
+    f = proj.clone()
+    engine.wbp(f, vol)
+    q, scale = engine.quantize(proj, F16)
+    engine.sirt_lp(q, scale, vol, 3, 0.5, "f16")
+    got = host(vol)
+    assert np.isfinite(got).all()
+    R = restatement
+    g = R.geom(nx, ny, nt, th, 1, 0, org)
+    p = host(proj)
+    ref = R.backproject(g, c8, R.filter_rweight(p), np.zeros((th, ny, nx)), fp64=True)
+    ref = R.sirt(g, c8, p, ref, 3, 0.5, fp64=True)
+    rel, mx = errors(got, ref)
+    print(f"WBP + SIRT-3 proj f16 resid f16 ({noise} noise): rel-L2 {rel:.3e}, max-abs {mx:.3e}")
+    assert rel < 1e-4
