@@ -14,6 +14,9 @@ Configurations (sizes are nx, ny, tilts, thickness):
 * ``cfg1`` -- SIRT-30, gamma 0.5: 61 tilts step 2, 1024x1024, volume
   1024x1024x256, 400 ellipsoids + 80 beads, per-tilt in-plane rotation
   N(0, 0.5 deg), XTILT 0.3 deg, noise 0.3 std, seed 1.
+* ``cfg2`` -- SIRT-20 in the Z layout with 16-bit storage: 61 tilts step 2,
+  4096x4096, volume 4096x4096x512, 3000 ellipsoids + 300 beads, ideal
+  single-axis geometry, Poisson counting noise at a mean of 20 e-/px, seed 2.
 
 Functions take ``scale`` to shrink a configuration (all lengths divided) for
 quick tests.  The phantom is built with torch on any device; projecting is
@@ -61,6 +64,12 @@ def config(name: str, scale: int = 1) -> Config:
         c = Config("cfg1", 1024, 1024, 256, np.arange(-60, 61, 2, dtype=np.float32),
                    400, 80, 1, xtilt=0.3, rotation_sigma=0.5, noise=0.3,
                    method="SIRT", iters=30, gamma=0.5)
+    elif name == "cfg2":
+        # Ideal single-axis geometry (no offsets, no XTILT): rows independent.
+        c = Config("cfg2", 4096, 4096, 512, np.arange(-60, 61, 2, dtype=np.float32),
+                   3000, 300, 2, method="SIRT", iters=20, gamma=0.5)
+        c.extra["scale"] = 0.5  # semi-axes U(8, 80) px, bead radius 6 px
+        c.extra["noise"] = "poisson"
     else:
         raise KeyError(name)
     if scale > 1:

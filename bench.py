@@ -415,6 +415,148 @@ def run_kernels(args):
     eng.close()
 
 
+def run_cfg0(args):
+    """WBP configuration (41 tilts, 256^2, volume 256x256x64): device-resident
+    filter + back-projection timed with CUDA events, the host-buffer call
+    end to end, and the reference's own CPU filter + BackProject (oracle/_ref,
+    one thread) on the same input, with the parity of the two volumes."""
+    import torch
+
+    import oracle
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+    build.build_lib()
+    torch.cuda.set_device(0)
+    cfg = synth.config("cfg0")
+    c8 = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    eng = T.Engine(0)
+    eng.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Y)
+    proj = synth.project_series(eng, cfg, 0, "gaussian")
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    work = proj.clone()
+    reps = 200
+    for _ in range(5):
+        work.copy_(proj)
+        eng.wbp(work, vol)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    for _ in range(reps):
+        work.copy_(proj)
+    c1.record()
+    e0.record()
+    for _ in range(reps):
+        work.copy_(proj)
+        eng.wbp(work, vol)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = (e0.elapsed_time(e1) - c0.elapsed_time(c1)) / reps
+    vpu = nt * nx * ny * th
+    proj_h = proj.cpu().pin_memory()
+    vol_h = torch.zeros((ny, th, nx)).pin_memory()
+    pn, vn = proj_h.numpy(), vol_h.numpy()
+    eng.reconstruct_host("WBP", pn.copy(), vn)
+    t0 = time.perf_counter()
+    for _ in range(20):
+        vn[...] = 0
+        eng.reconstruct_host("WBP", pn.copy(), vn)
+    e2e_ms = (time.perf_counter() - t0) / 20 * 1e3
+    ours = vn.copy()
+    ref = {"available": oracle.reference_available()}
+    if ref["available"]:
+        R = oracle.Reference()
+        c20 = oracle.coeff20(c8)
+        p_np = proj.cpu().numpy()
+        t0 = time.perf_counter()
+        f = R.filter_rweight(p_np)
+        rv = R.y_backproject(nx, ny, nt, th, c20, (nx * 0.5, th * 0.5, th * 0.5), f,
+                             np.zeros((ny, th, nx), np.float32))
+        ref_s = time.perf_counter() - t0
+        ref.update({"value": vpu / ref_s, "seconds": ref_s, "cores": 1,
+                    "kind": "reference", "rel_l2_ours_vs_reference": oracle.rel_l2(ours, rv)})
+    eng.close()
+    print(json.dumps({"workload": "cfg0", "metric": "voxel-proj updates/s", "unit": "VPU/s",
+                      "value": vpu / (ms / 1e3), "ms_per_reconstruction": ms,
+                      "e2e": {"value": vpu / (e2e_ms / 1e3), "ms": e2e_ms,
+                              "h2d_bytes": int(pn.nbytes + vn.nbytes),
+                              "d2h_bytes": int(vn.nbytes)},
+                      "cpu_reference": ref, "dtype": "f32", "data": "synthetic",
+                      "config": {"method": "WBP", "tilts": nt, "proj": [ny, nx],
+                                 "volume": [nx, ny, th], "layout": "Y"}}), flush=True)
+
+
+def run_cfg2(args):
+    """Mixed-precision configuration: SIRT-20 in the Z layout, 61 tilts of
+    4096^2, volume 4096x4096x512 (34 GB), counting noise; FP16 projections and
+    residuals with FP32 volume and sums, beside the plain FP32 form on the same
+    GPU.  Error against the FP64 oracle on a band of rows (the ideal geometry
+    makes rows independent, so the band is an exact sub-problem)."""
+    import torch
+
+    import oracle
+    from autom2_b200 import build, synth
+    from autom2_b200 import tiltrec as T
+    build.build_lib()
+    torch.cuda.set_device(0)
+    cfg = synth.config("cfg2")
+    c8 = synth.coefficients(cfg)
+    nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
+    org = T.default_origin(T.LAYOUT_Z, nx, ny, th)
+    eng = T.Engine(0)
+    eng.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Z, org)
+    t0 = time.perf_counter()
+    proj = synth.project_series(eng, cfg, T.LAYOUT_Z, "poisson")
+    gen_s = time.perf_counter() - t0
+    vol = torch.zeros((th, ny, nx), device="cuda")
+    iters = args.iters if args.iters != 2 else cfg.iters
+    vpu = 2.0 * iters * nt * nx * ny * th
+
+    def timed(fn):
+        vol.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    eng.sirt(proj, vol, 1, cfg.gamma)  # weights, warm
+    t_f32 = timed(lambda: eng.sirt(proj, vol, iters, cfg.gamma))
+    band = 4
+    r0 = ny // 2 - band // 2
+    f32_band = vol[:, r0:r0 + band].cpu().numpy()
+    q, scale = eng.quantize(proj, torch.float16)
+    t_lp = timed(lambda: eng.sirt_lp(q, scale, vol, iters, cfg.gamma, "f16"))
+    lp_band = vol[:, r0:r0 + band].cpu().numpy()
+    p_band = proj[:, r0:r0 + band].cpu().numpy()
+    eng.close()
+    R = oracle.Restatement()
+    g = R.geom(nx, band, nt, th, T.LAYOUT_Z, 0, (org[0], org[1] - r0, org[2]))
+    t0 = time.perf_counter()
+    ref = R.sirt(g, c8, p_band, np.zeros((th, band, nx)), iters, cfg.gamma, fp64=True)
+    oracle_s = time.perf_counter() - t0
+
+    def err(a):
+        a64 = np.asarray(a, np.float64)
+        return {"rel_l2": oracle.rel_l2(a64, ref),
+                "max_abs_rel": float(np.abs(a64 - ref).max() / np.abs(ref).max())}
+
+    print(json.dumps({"workload": "cfg2", "metric": "voxel-proj updates/s", "unit": "VPU/s",
+                      "value": vpu / t_lp, "seconds": t_lp,
+                      "dtype": "f16 storage (projections, residual), f32 volume and sums",
+                      "vs_fp64_oracle": err(lp_band),
+                      "plain_f32": {"value": vpu / t_f32, "seconds": t_f32,
+                                    "vs_fp64_oracle": err(f32_band)},
+                      "oracle": {"rows": [r0, r0 + band], "seconds": oracle_s},
+                      "generation_s": gen_s, "data": "synthetic",
+                      "config": {"method": f"SIRT-{iters}", "tilts": nt, "proj": [ny, nx],
+                                 "volume": [nx, ny, th], "layout": "Z",
+                                 "noise": "Poisson, mean 20 e-/px"}}), flush=True)
+
+
 class OutputPool:
     """Reusable output volumes per projection size (the batch and serving
     runs keep only this many results alive at once)."""
@@ -659,7 +801,8 @@ def main():
                     help="profiling case only (see run_kernels)")
     ap.add_argument("--scale", type=int, default=2)
     ap.add_argument("--iters", type=int, default=2)
-    ap.add_argument("--workload", default="sirt", choices=["sirt", "batch", "serve"],
+    ap.add_argument("--workload", default="sirt",
+                    choices=["sirt", "cfg0", "cfg2", "batch", "serve"],
                     help="sirt: the headline SIRT-30 line; batch / serve: the batched "
                          "and serving configurations (one JSON line each)")
     ap.add_argument("--jobs", type=int, default=0)
@@ -668,7 +811,11 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--storage", default="f16", choices=["f32", "f16", "bf16"])
     args = ap.parse_args()
-    if args.workload == "batch":
+    if args.workload == "cfg0":
+        run_cfg0(args)
+    elif args.workload == "cfg2":
+        run_cfg2(args)
+    elif args.workload == "batch":
         run_batch(args)
     elif args.workload == "serve":
         run_serve(args)
