@@ -3,7 +3,7 @@
 // Same flags and files as the reference executables:
 //   --input/-i <mrc>   --output/-o <mrc>   --tiltfile/-t <angles>
 //   --geometry/-g offset,pitch,zshift,thickness
-//   --method/-m BPT | WBP | SIRT,n,gamma | SART,n,gamma   (FBP, ADMM: see below)
+//   --method/-m BPT | FBP | WBP | SIRT,n,gamma | SART,n,gamma   (ADMM: see below)
 //   --inital/-n <mrc> (cuda dialect, sic) or --initial <mrc> (mpi dialect)
 //   --axis/-a y|z (parsed; the executable name selects the layout)
 //   --f2b/-f (byte output)   --help/-h
@@ -22,8 +22,9 @@
 // Differences, all deliberate: --initial is honoured on the GPU path (the
 // reference GPU code parses it and ignores it, recon_y.cu:345); a bare
 // SIRT/SART without iterations is an error (the reference leaves them
-// uninitialised, opts.cpp:112-123); FBP filter modes 0/1 and ADMM report that
-// they are not provided; errors exit with status 1.
+// uninitialised, opts.cpp:112-123); ADMM reports that it is not provided;
+// errors exit with status 1.  FBP is the Shepp-Logan filter (ApplyFilterInplace
+// mode 0, main-mpi.cpp:835-839) then the back-projection.
 #include <getopt.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -63,7 +64,7 @@ void usage() {
       "  --tiltfile(-t) <file>    tilt angles, degrees\n"
       "  --inital(-n)/--initial <mrc>  starting volume\n"
       "  --geometry(-g) offset,pitch_angle,zshift,thickness\n"
-      "  --method(-m) BPT | WBP | SIRT,iterations,relax | SART,iterations,relax\n"
+      "  --method(-m) BPT | FBP | WBP | SIRT,iterations,relax | SART,iterations,relax\n"
       "  --f2b(-f)                write bytes (0-255)\n"
       "  --help(-h)\n"
       "example: mpirun -n 1 ./%s --input a.mrc --output v.mrc --tiltfile a.rawtlt"
@@ -195,13 +196,15 @@ int run(const Options &o) {
     method = TR_METHOD_BPT;
   else if (o.method == "WBP")
     method = TR_METHOD_WBP;
+  else if (o.method == "FBP")
+    method = TR_METHOD_FBP;
   else if (o.method == "SIRT" || o.method == "SART") {
     if (o.iteration < 0)
       return fprintf(stderr, "%s: %s needs iterations and relaxation (%s,n,gamma)\n", kProg,
                      o.method.c_str(), o.method.c_str()),
              1;
     method = o.method == "SIRT" ? TR_METHOD_SIRT : TR_METHOD_SART;
-  } else if (o.method == "FBP" || o.method == "ADMM") {
+  } else if (o.method == "ADMM") {
     return fprintf(stderr, "%s: method %s is not provided by this engine\n", kProg,
                    o.method.c_str()),
            1;
@@ -225,8 +228,8 @@ int run(const Options &o) {
   std::vector<float> proj((size_t)nx * ny * nt);
   // Byte stacks: the Y executables read through ReadBlock (signed); the Z
   // executables read BPT/SIRT/SART projections through ReadSliceZ
-  // (unsigned) and WBP through ReadBlock (signed).
-  const bool signed_bytes = !zlayout || method == TR_METHOD_WBP;
+  // (unsigned) and WBP / FBP through ReadBlock (signed, main-mpiz.cpp:365-384).
+  const bool signed_bytes = !zlayout || method == TR_METHOD_WBP || method == TR_METHOD_FBP;
   if (!trcli::read_sections(o.input, in, 0, nt, signed_bytes, proj.data(), &err))
     return fprintf(stderr, "%s\n", err.c_str()), 1;
 
@@ -241,7 +244,8 @@ int run(const Options &o) {
   // (main-mpi.cpp:778-791); the Z-layout BPT/WBP start from zero
   // (main-mpiz.cpp BackProject/FBP zero the volume).
   const bool use_initial = !o.initial.empty() &&
-                           !(zlayout && (method == TR_METHOD_BPT || method == TR_METHOD_WBP));
+                           !(zlayout && (method == TR_METHOD_BPT || method == TR_METHOD_WBP ||
+                                         method == TR_METHOD_FBP));
   if (use_initial) {
     trcli::MrcHeader ih;
     if (!trcli::read_header(o.initial, &ih, &err)) return fprintf(stderr, "%s\n", err.c_str()), 1;

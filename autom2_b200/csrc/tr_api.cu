@@ -463,6 +463,26 @@ tr_status tr_filter_rweight(tr_ctx *c, float *proj, void *stream) {
   return TR_OK;
 }
 
+tr_status tr_filter_fbp(tr_ctx *c, float *proj, int mode, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || (mode != 0 && mode != 1))
+    return fail(c, TR_ERR_ARG, "bad FBP filter arguments (mode %d)", mode);
+  // DFT length of the reference: the smallest 2^a 3^b 5^c >= 251 + (nx + 2) - 1
+  // (cvGetOptimalDFTSize).
+  int L = c->nx + 252;
+  for (;; ++L) {
+    int r = L;
+    while (r % 2 == 0) r /= 2;
+    while (r % 3 == 0) r /= 3;
+    while (r % 5 == 0) r /= 5;
+    if (r == 1) break;
+  }
+  TR_CUDA(c, launch_fbp_filter(proj, (long long)c->ny * c->nt, c->nx, L, mode,
+                               (cudaStream_t)stream));
+  return TR_OK;
+}
+
 tr_status tr_backproject(tr_ctx *c, const float *proj, float *vol, int z0, int nz,
                          void *stream) {
   tr_status st = need_problem(c);
@@ -709,6 +729,10 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   switch (method) {
     case TR_METHOD_BPT: st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s); break;
     case TR_METHOD_WBP: st = tr_wbp(c, c->hproj_d, c->hvol_d, s); break;
+    case TR_METHOD_FBP:
+      st = tr_filter_fbp(c, c->hproj_d, 0, s);
+      if (!st) st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s);
+      break;
     case TR_METHOD_SIRT: st = tr_sirt(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
     case TR_METHOD_SART: st = tr_sart(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
     default: st = fail(c, TR_ERR_ARG, "unknown method %d", method);

@@ -21,6 +21,8 @@
 // rows at once because the kernel is real.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "tr_internal.cuh"
 
 namespace trb {
@@ -104,6 +106,79 @@ cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s) {
   const long long pairs = (f.nrows + 1) / 2;
   const int threads = M >= 8192 ? 512 : 256;
   rweight_kernel<<<(unsigned)pairs, threads, smem, s>>>(f);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------- FBP filters
+//
+// FBP row filters, ApplyFilterInplace modes 0 (Shepp-Logan) and 1 (Ram-Lak)
+// (filter/filter_prj.cpp:755-786): FileterProjectionSymmetrize (:265-446)
+// convolves each row, padded by one edge sample on each side and extended by
+// mirroring to the DFT length L = optimal(251 + nx + 1), with a 251-tap kernel
+// through forward DFTs, a spectrum product and a scaled inverse, and keeps
+// samples [126, 126 + nx) of the circular result.  That is
+//   out[i] = sum_{k<251} f[k] x[(126 + i - k) mod L],
+// evaluated here as a direct sum in double precision (251 products per
+// output; the kernel's many small taps make float accumulation lose ~1e-6).
+// One CTA per row: the row's extended samples e[t] = x[(t - 124) mod L],
+// t in [0, nx + 250], and the taps live in shared memory.
+
+constexpr int kFbpTaps = 251;
+
+__global__ void __launch_bounds__(256) fbp_filter_kernel(float *rows, int nx, int L, int mode) {
+  extern __shared__ double fsm[];
+  double *f = fsm;                                     // [251]
+  float *e = reinterpret_cast<float *>(fsm + kFbpTaps);  // [nx + 250]
+  const int half = kFbpTaps / 2;
+  for (int k = threadIdx.x; k < kFbpTaps; k += blockDim.x) {
+    // The reference's kernels, formed in the same precision (:137-178).
+    const double pi = 3.14159265358979323846;
+    float v;
+    if (mode == 1) {
+      const int n = k - half;
+      v = n == 0 ? (float)(pi / 4) : ((n % 2) != 0 ? (float)(-1.0 / (pi * n * n)) : 0.f);
+    } else {
+      const double n = (double)((float)(k - half));
+      v = (float)(-2.0 / (pi * (4.0 * n * n - 1.0)));
+    }
+    f[k] = (double)v;
+  }
+  float *r = rows + (size_t)blockIdx.x * nx;
+  const int np = nx + 2;
+  const int end = np >= L - np ? L : 2 * np;  // mirrored extension, zeros after
+  for (int t = threadIdx.x; t < nx + kFbpTaps - 1; t += blockDim.x) {
+    int m = t - (half - 1);
+    if (m < 0) m += L;
+    // x[m] of the padded, extended row
+    int src;  // index into the padded row [0, np)
+    if (m < np) src = m;
+    else if (m < end) src = 2 * np - 1 - m;
+    else src = -1;
+    float v = 0.f;
+    if (src >= 0) v = r[min(max(src - 1, 0), nx - 1)];
+    e[t] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+    double acc = 0.0;
+    const float *w = e + i + kFbpTaps - 1;
+#pragma unroll 8
+    for (int k = 0; k < kFbpTaps; ++k) acc = fma(f[k], (double)w[-k], acc);
+    // All reads of the row precede this write: e is a private copy.
+    r[i] = (float)acc;
+  }
+}
+
+cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int mode,
+                              cudaStream_t s) {
+  const size_t smem = kFbpTaps * sizeof(double) + (size_t)(nx + kFbpTaps) * sizeof(float);
+  cudaError_t e = cudaFuncSetAttribute(fbp_filter_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  for (long long r0 = 0; r0 < nrows; r0 += 2147483647ll) {
+    const unsigned n = (unsigned)std::min<long long>(nrows - r0, 2147483647ll);
+    fbp_filter_kernel<<<n, 256, smem, s>>>(rows + (size_t)r0 * nx, nx, L, mode);
+  }
   return cudaGetLastError();
 }
 

@@ -196,6 +196,8 @@ cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const fl
                             const float *wt, size_t plane, int nt, int rdtype, void *r,
                             const float *rs, int nsm, cudaStream_t s);
 cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
+cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int mode,
+                              cudaStream_t s);
 dim3 bp_tile_grid(const VolView &v);
 dim3 fp_tile_grid(const VolView &v);
 bool batch_bp_layout(const BpArgs &a0, bool sep, size_t budget, BatchBp *out, size_t *smem);

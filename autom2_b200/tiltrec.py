@@ -34,9 +34,9 @@ import numpy as np
 from . import build as _build
 
 LAYOUT_Y, LAYOUT_Z = 0, 1
-METHOD_BPT, METHOD_WBP, METHOD_SIRT, METHOD_SART = 0, 1, 2, 3
+METHOD_BPT, METHOD_WBP, METHOD_SIRT, METHOD_SART, METHOD_FBP = 0, 1, 2, 3, 4
 METHODS = {"BPT": METHOD_BPT, "WBP": METHOD_WBP, "SIRT": METHOD_SIRT,
-           "SART": METHOD_SART}
+           "SART": METHOD_SART, "FBP": METHOD_FBP}
 DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
 DTYPES = {"f32": DTYPE_F32, "f16": DTYPE_F16, "bf16": DTYPE_BF16}
 
@@ -88,6 +88,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_set_problem.argtypes = [vp, i, i, i, i, i, dp, f, f, f]
     lib.tr_update_geometry.argtypes = [vp, dp, vp]
     lib.tr_filter_rweight.argtypes = [vp, vp, vp]
+    lib.tr_filter_fbp.argtypes = [vp, vp, i, vp]
     lib.tr_backproject.argtypes = [vp, vp, vp, i, i, vp]
     lib.tr_forward_project.argtypes = [vp, vp, i, i, vp, vp, vp]
     lib.tr_sirt.argtypes = [vp, vp, vp, i, f, vp]
@@ -205,6 +206,11 @@ class Engine:
     def filter_rweight(self, proj):
         self._check(self.lib.tr_filter_rweight(self.h, _ptr(proj), _stream(self.device)),
                     "tr_filter_rweight")
+
+    def filter_fbp(self, proj, mode=0):
+        """FBP row filter in place: mode 0 Shepp-Logan, 1 Ram-Lak."""
+        self._check(self.lib.tr_filter_fbp(self.h, _ptr(proj), mode, _stream(self.device)),
+                    "tr_filter_fbp")
 
     def backproject(self, proj, vol, z0=0, nz=None):
         nz = self.shape[3] - z0 if nz is None else nz

@@ -60,7 +60,8 @@ typedef enum {
   TR_METHOD_BPT = 0,   /* back-projection                    (--method BPT) */
   TR_METHOD_WBP = 1,   /* R-weighting filter + BPT           (--method WBP) */
   TR_METHOD_SIRT = 2,  /* SIRT,n,gamma                       */
-  TR_METHOD_SART = 3   /* SART,n,gamma                       */
+  TR_METHOD_SART = 3,  /* SART,n,gamma                       */
+  TR_METHOD_FBP = 4    /* Shepp-Logan FBP filter + BPT       (--method FBP) */
 } tr_method;
 
 /* Element types of 16-bit storage (projections, SIRT residuals). */
@@ -109,6 +110,14 @@ tr_status tr_update_geometry(tr_ctx *ctx, const double *coeff8, void *stream);
  * ApplyFilterInplace(..., mode 2) (src/TiltRec/src/filter/filter_prj.h:24,
  * filter_prj.cpp:674-736, 787-795). */
 tr_status tr_filter_rweight(tr_ctx *ctx, float *proj_dev, void *stream);
+
+/* FBP row filter in place over every row of the stack: ApplyFilterInplace
+ * modes 0 (Shepp-Logan) and 1 (Ram-Lak) (filter_prj.cpp:755-786), i.e.
+ * FileterProjectionSymmetrize (:265-446) with the 251-tap kernels of
+ * :137-178: each row, edge-padded and mirror-extended to the reference's DFT
+ * length, circularly convolved with the kernel; computed as a direct sum in
+ * double precision. */
+tr_status tr_filter_fbp(tr_ctx *ctx, float *proj_dev, int mode, void *stream);
 
 /* vol += sum over tilts of s/c (normalised bilinear gather) on sections
  * [z0, z0+nz) of the volume; vol_dev points at section z0 of the layout's

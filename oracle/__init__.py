@@ -66,6 +66,8 @@ class Restatement:
         lib.orc_coeffs.argtypes = [_f32p, C.c_int, C.c_float, C.c_float,
                                    C.c_float, _f64p]
         lib.orc_filter_rweight.argtypes = [C.c_int, C.c_long, _f32p]
+        lib.orc_filter_fbp.argtypes = [C.c_int, C.c_int, C.c_long, _f32p]
+        lib.orc_optimal_dft_size.argtypes = [C.c_int]
         for pfx, p in (("orc_", _f32p), ("orc64_", _f64p)):
             real = C.c_float if pfx == "orc_" else C.c_double
             g = C.POINTER(Geom)
@@ -92,6 +94,16 @@ class Restatement:
         nx = p.shape[-1]
         self.lib.orc_filter_rweight(nx, p.size // nx, p)
         return p
+
+    def filter_fbp(self, proj, mode=0):
+        """FBP row filter (mode 0 Shepp-Logan, 1 Ram-Lak) of a copy of proj."""
+        p = _c(proj, np.float32).copy()
+        nx = p.shape[-1]
+        self.lib.orc_filter_fbp(mode, nx, p.size // nx, p)
+        return p
+
+    def optimal_dft_size(self, n):
+        return int(self.lib.orc_optimal_dft_size(n))
 
     def _pfx(self, fp64):
         return ("orc64_", np.float64) if fp64 else ("orc_", np.float32)

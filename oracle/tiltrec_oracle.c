@@ -124,3 +124,77 @@ void orc_filter_rweight(int nx, long nrows, float *rows) {
 #include "tiltrec_oracle_impl.h"
 #undef PFX
 #undef REAL
+
+int orc_optimal_dft_size(int n) {
+  for (int m = n > 1 ? n : 1;; ++m) {
+    int r = m;
+    while (r % 2 == 0) r /= 2;
+    while (r % 3 == 0) r /= 3;
+    while (r % 5 == 0) r /= 5;
+    if (r == 1) return m;
+  }
+}
+
+/* The filter kernels as filter_prj.cpp forms them (float arithmetic):
+ * RamLak(251): n = -125..125, pi/4 at n = 0, -1/(pi n^2) at odd n, 0 at even
+ * n (:137-155); SheppLogan(251): -2/(pi (4 n^2 - 1)) with float n (:158-178).
+ *
+ * FileterProjectionSymmetrize per row (the y padding rows are filtered and
+ * cropped away, so rows are independent): the row is padded by one sample on
+ * each side with its edge values (the 2-D symmetrisation about the centred
+ * ROI, :301-316 with :209-263); that padded row of n = nx + 2 samples is
+ * extended to L = optimal(251 + n - 1) by mirroring about its right end
+ * (x[i] = x[2n - 1 - i], up to 2n, zeros beyond; :370-389); the kernel sits at
+ * [0, 251) of an L-sample buffer; forward DFTs, a spectrum product and the
+ * scaled inverse give the circular convolution y = kernel (*) x; samples
+ * [125, 125 + n) of y are the filtered padded row (:397-401), whose centre
+ * [1, 1 + nx) is the output (:403-413).  So out[i] = sum_k f[k] x[(126 + i -
+ * k) mod L]. */
+int orc_filter_fbp(int mode, int nx, long nrows, float *rows) {
+  const int len = 251, half = len / 2;
+  float f[251];
+  if (mode == 1) {
+    int n = -(len - 1) / 2;
+    for (int i = 0; i < len; ++i, ++n) {
+      if (n == 0)
+        f[i] = (float)(3.14159265358979323846 / 4);
+      else if (abs(n % 2) == 1)
+        f[i] = (float)(-1.0 / (3.14159265358979323846 * n * n));
+      else
+        f[i] = 0;
+    }
+  } else {
+    float n = -((float)len - 1.0f) / 2.0f;
+    for (int i = 0; i < len; ++i) {
+      f[i] = (float)(-2.0 / (3.14159265358979323846 * (4.0 * n * n - 1.0)));
+      n = n + 1.0f;
+    }
+  }
+  const int np = nx + 2;
+  const int L = orc_optimal_dft_size(len + np - 1);
+#pragma omp parallel
+  {
+    float *x = (float *)calloc((size_t)L, sizeof(float));
+#pragma omp for schedule(static)
+    for (long row = 0; row < nrows; ++row) {
+      float *r = rows + (size_t)row * nx;
+      for (int i = 0; i < L; ++i) x[i] = 0;
+      x[0] = r[0];
+      for (int i = 0; i < nx; ++i) x[1 + i] = r[i];
+      x[np - 1] = r[nx - 1];
+      const int end = np >= L - np ? L : 2 * np;
+      for (int i = np; i < end; ++i) x[i] = x[2 * np - 1 - i];
+      for (int i = 0; i < nx; ++i) {
+        double acc = 0;
+        for (int k = 0; k < len; ++k) {
+          int m = (half + 1 + i - k) % L;
+          if (m < 0) m += L;
+          acc += (double)f[k] * (double)x[m];
+        }
+        r[i] = (float)acc;
+      }
+    }
+    free(x);
+  }
+  return L;
+}

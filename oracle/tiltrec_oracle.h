@@ -41,6 +41,18 @@ void orc_coeffs(const float *angles, int nt, float offset, float pitch,
  * convolution on the padded row. */
 void orc_filter_rweight(int nx, long nrows, float *rows);
 
+/* FBP row filters, modes 0 (Shepp-Logan) and 1 (Ram-Lak) of
+ * ApplyFilterInplace (filter_prj.cpp:755-786), in place over nrows rows of nx
+ * floats: FileterProjectionSymmetrize (:265-446) with its 251-tap kernel
+ * (RamLak :137-155, SheppLogan :158-178), evaluated as the circular
+ * convolution its DFTs compute, in double precision.  Returns the DFT length
+ * L the reference would use. */
+int orc_filter_fbp(int mode, int nx, long nrows, float *rows);
+
+/* Smallest integer >= n whose only prime factors are 2, 3 and 5 (the
+ * sizes OpenCV's getOptimalDFTSize returns). */
+int orc_optimal_dft_size(int n);
+
 #define ORC_DECLARE(PFX, REAL)                                                \
   void PFX##backproject(const orc_geom *g, const double *coeff8,              \
                         const REAL *proj, REAL *vol);                          \

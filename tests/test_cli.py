@@ -40,7 +40,7 @@ def test_argument_errors(exes, tmp_path):
     assert r.returncode == 1 and "thickness" in r.stderr
     r = run(exe, *base, "-g", "0,0,0,4", "-m", "SIRT")
     assert r.returncode == 1 and "needs iterations" in r.stderr
-    r = run(exe, *base, "-g", "0,0,0,4", "-m", "FBP")
+    r = run(exe, *base, "-g", "0,0,0,4", "-m", "ADMM,2,3,0.5,0.01")
     assert r.returncode == 1 and "not provided" in r.stderr
     r = run(exe, *base, "-g", "0,0,0,4,9", "-m", "BPT")
     assert r.returncode == 1

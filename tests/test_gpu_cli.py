@@ -108,6 +108,8 @@ def restated(layout, proj, ang, geometry, method):
         return R.backproject(g, c8, proj, zero)
     if parts[0] == "WBP":
         return R.backproject(g, c8, R.filter_rweight(proj), zero)
+    if parts[0] == "FBP":
+        return R.backproject(g, c8, R.filter_fbp(proj, 0), zero)
     f = R.sirt if parts[0] == "SIRT" else R.sart
     return f(g, c8, proj, zero, int(parts[1]), float(parts[2]))
 
@@ -133,6 +135,22 @@ def test_tiltrecz_vs_tiltrecz_mpi(case, method):
     ours(1, *common, "--output", str(a))
     reference(1, *common, "--output", str(b))
     compare(a, b)
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_fbp_vs_oracle(case, restatement, layout):
+    """--method FBP: the reference's FBP filter needs OpenCV, which the
+    reference build here stubs out, so the executables are checked against the
+    oracle restatement (its filter is pinned to the reference's DFT steps in
+    test_oracle_pin.py)."""
+    d, proj, ang = case
+    th = 10
+    out = d / f"fbp_{layout}.mrc"
+    geometry = f"0.5,{0 if layout else 1.5},0,{th}"
+    ours(layout, "--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+         "--geometry", geometry, "--method", "FBP", "--output", str(out))
+    _, _, got = read_mrc(out)
+    assert O.rel_l2(got, restated(layout, proj, ang, geometry, "FBP")) < TOL
 
 
 @pytest.mark.parametrize("method,iters", [("BPT", 0), ("SIRT", 2)])

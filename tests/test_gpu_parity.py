@@ -229,3 +229,34 @@ def test_errors_are_reported(engine):
                    torch.zeros((64, 8, 64), device="cuda"), 1, 0.5)
     assert e.value.status == -3  # TR_ERR_BUDGET
     small.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("nx", [64, 300, 1024, 4096])
+def test_fbp_filter_widths(engine, restatement, nx, mode):
+    """FBP row filters (Shepp-Logan, Ram-Lak) against the oracle's double
+    sum; both branches of the reference's mirrored extension (short rows)."""
+    rng = np.random.default_rng(nx * 3 + mode)
+    rows = rng.normal(size=(2, 5, nx)).astype(np.float32)
+    c8 = restatement.coeffs(np.zeros(2, np.float32))
+    engine.set_problem(nx, 5, 2, 4, c8, 0)
+    p = dev(rows)
+    engine.filter_fbp(p, mode)
+    want = restatement.filter_fbp(rows, mode)
+    got = host(p)
+    assert O.rel_l2(got, want) < 1e-6
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_fbp_reconstruction(engine, restatement, layout):
+    """--method FBP: Shepp-Logan filter then the back-projection, through the
+    host-buffer call, against the oracle."""
+    R = restatement
+    nx, ny, nt, th, c8, proj, vol0, org = _random_case(R, "xtilt", layout)
+    engine.set_problem(nx, ny, nt, th, c8, layout, org)
+    vol = np.zeros(vol0.shape, np.float32)
+    engine.reconstruct_host("FBP", proj.copy(), vol)
+    g = R.geom(nx, ny, nt, th, layout, 0, org)
+    want = R.backproject(g, c8, R.filter_fbp(proj, 0), np.zeros(vol0.shape, np.float32))
+    assert O.rel_l2(vol, want) < TOL

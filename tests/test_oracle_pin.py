@@ -139,3 +139,57 @@ def test_reference_live_random_case(reference, restatement):
     np.testing.assert_array_equal(
         restatement.sirt(g, c8, proj, vol, 2, 0.3),
         reference.y_sirt(nx, ny, nt, th, O.coeff20(c8), org, proj, vol, 2, 0.3))
+
+
+def _fbp_by_dft(row, taps):
+    """The reference's FBP row filter step by step with numpy's FFT
+    (FileterProjectionSymmetrize, filter_prj.cpp:265-446): edge-padded row,
+    mirrored extension to the optimal DFT length, spectrum product with the
+    251-tap kernel, scaled inverse, samples [126, 126 + nx)."""
+    nx = row.size
+    n = nx + 2
+    length = len(taps)
+    big = n + length - 1
+    L = big
+    while True:
+        r = L
+        for q in (2, 3, 5):
+            while r % q == 0:
+                r //= q
+        if r == 1:
+            break
+        L += 1
+    x = np.zeros(L)
+    x[1:nx + 1] = row
+    x[0], x[n - 1] = row[0], row[-1]
+    end = L if n >= L - n else 2 * n
+    for i in range(n, end):
+        x[i] = x[2 * n - 1 - i]
+    f = np.zeros(L)
+    f[:length] = taps
+    y = np.fft.ifft(np.fft.fft(x) * np.fft.fft(f)).real
+    return y[length // 2 + 1: length // 2 + 1 + nx], L
+
+
+def _taps(mode):
+    n = np.arange(-125, 126)
+    if mode == 1:
+        t = np.where(n == 0, np.pi / 4, np.where(np.abs(n) % 2 == 1, -1.0 / (np.pi * n * n + (n == 0)), 0.0))
+        return t.astype(np.float32).astype(np.float64)
+    return (-2.0 / (np.pi * (4.0 * n.astype(np.float32).astype(np.float64) ** 2 - 1.0))
+            ).astype(np.float32).astype(np.float64)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("nx", [64, 300, 1024])
+def test_fbp_filter_restatement_matches_dft_steps(restatement, mode, nx):
+    """The restatement's direct sum equals the reference's DFT steps (numpy
+    FFT in double) on the same row, for both branches of the mirrored
+    extension (short rows mirror only up to twice their length)."""
+    rng = np.random.default_rng(nx + mode)
+    rows = rng.normal(size=(3, nx)).astype(np.float32)
+    got = restatement.filter_fbp(rows, mode)
+    for r in range(3):
+        want, L = _fbp_by_dft(rows[r].astype(np.float64), _taps(mode))
+        assert L == restatement.optimal_dft_size(nx + 2 + 250)
+        assert np.abs(got[r] - want).max() <= 1e-5 * np.abs(want).max()
