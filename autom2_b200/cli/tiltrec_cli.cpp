@@ -3,7 +3,7 @@
 // Same flags and files as the reference executables:
 //   --input/-i <mrc>   --output/-o <mrc>   --tiltfile/-t <angles>
 //   --geometry/-g offset,pitch,zshift,thickness
-//   --method/-m BPT | FBP | WBP | SIRT,n,gamma | SART,n,gamma   (ADMM: see below)
+//   --method/-m BPT | FBP | WBP | SIRT,n,gamma | SART,n,gamma | ADMM,n,cg,mu,soft
 //   --inital/-n <mrc> (cuda dialect, sic) or --initial <mrc> (mpi dialect)
 //   --axis/-a y|z (parsed; the executable name selects the layout)
 //   --f2b/-f (byte output)   --help/-h
@@ -22,8 +22,8 @@
 // Differences, all deliberate: --initial is honoured on the GPU path (the
 // reference GPU code parses it and ignores it, recon_y.cu:345); a bare
 // SIRT/SART without iterations is an error (the reference leaves them
-// uninitialised, opts.cpp:112-123); ADMM reports that it is not provided;
-// errors exit with status 1.  FBP is the Shepp-Logan filter (ApplyFilterInplace
+// uninitialised, opts.cpp:112-123); ADMM (TiltRecZ-mpi only in the reference)
+// runs in both layouts; errors exit with status 1.  FBP is the Shepp-Logan filter (ApplyFilterInplace
 // mode 0, main-mpi.cpp:835-839) then the back-projection.
 #include <getopt.h>
 #include <stdio.h>
@@ -51,9 +51,13 @@ struct Options {
   int thickness = 0;
   int iteration = -1;
   float gamma = 0;
+  int cgiter = -1;   // ADMM
+  float soft = 0;    // ADMM
   bool f2b = false;
 };
 
+// ADMM has no tr_method code: it takes two more parameters (tr_admm_host).
+constexpr int kMethodAdmm = -1;
 const char *kProg = TR_CLI_LAYOUT == 0 ? "TiltRec-cuda" : "TiltRecZ-cuda";
 
 void usage() {
@@ -65,6 +69,7 @@ void usage() {
       "  --inital(-n)/--initial <mrc>  starting volume\n"
       "  --geometry(-g) offset,pitch_angle,zshift,thickness\n"
       "  --method(-m) BPT | FBP | WBP | SIRT,iterations,relax | SART,iterations,relax\n"
+      "               | ADMM,iterations,cgiter,relax,soft\n"
       "  --f2b(-f)                write bytes (0-255)\n"
       "  --help(-h)\n"
       "example: mpirun -n 1 ./%s --input a.mrc --output v.mrc --tiltfile a.rawtlt"
@@ -134,9 +139,11 @@ int parse(int argc, char **argv, Options *o) {
           if (getline(iss, t, ',')) o->iteration = atoi(t.c_str());
           if (getline(iss, t)) o->gamma = (float)atof(t.c_str());
         } else if (o->method == "ADMM") {
-          // ADMM,iterations,cgiter,relax,soft: parsed, not provided.
-          while (getline(iss, t, ',')) {
-          }
+          // ADMM,iterations,cgiter,relax,soft (opts.cpp:301-311)
+          if (getline(iss, t, ',')) o->iteration = atoi(t.c_str());
+          if (getline(iss, t, ',')) o->cgiter = (int)atof(t.c_str());
+          if (getline(iss, t, ',')) o->gamma = (float)atof(t.c_str());
+          if (getline(iss, t)) o->soft = (float)atof(t.c_str());
         }
         break;
       }
@@ -205,9 +212,9 @@ int run(const Options &o) {
              1;
     method = o.method == "SIRT" ? TR_METHOD_SIRT : TR_METHOD_SART;
   } else if (o.method == "ADMM") {
-    return fprintf(stderr, "%s: method %s is not provided by this engine\n", kProg,
-                   o.method.c_str()),
-           1;
+    if (o.iteration < 0 || o.cgiter < 0)
+      return fprintf(stderr, "%s: ADMM needs ADMM,iterations,cgiter,relax,soft\n", kProg), 1;
+    method = kMethodAdmm;
   } else {
     return fprintf(stderr, "%s: unknown method '%s'\n", kProg, o.method.c_str()), 1;
   }
@@ -265,8 +272,10 @@ int run(const Options &o) {
     return fprintf(stderr, "%s: no CUDA device %d\n", kProg, device), 1;
   int st = tr_set_problem(ctx, nx, ny, nt, th, zlayout ? TR_LAYOUT_Z : TR_LAYOUT_Y, coeff.data(),
                           ox, oy, oz);
-  if (st == TR_OK) st = tr_reconstruct_host(ctx, method, proj.data(), vol.data(), o.iteration,
-                                            o.gamma);
+  if (st == TR_OK)
+    st = method == kMethodAdmm
+             ? tr_admm_host(ctx, proj.data(), vol.data(), o.iteration, o.cgiter, o.gamma, o.soft)
+             : tr_reconstruct_host(ctx, method, proj.data(), vol.data(), o.iteration, o.gamma);
   if (st != TR_OK) {
     fprintf(stderr, "%s: %s\n", kProg, tr_last_error(ctx));
     tr_destroy(ctx);

@@ -48,6 +48,8 @@ struct tr_ctx {
   void *res16_d = nullptr;      // 16-bit SIRT residual [ntilt][ny][nx]
   unsigned *maxbits_d = nullptr;  // per-tilt |p| maxima for tr_quantize
   float *rscale_d = nullptr;      // per-tilt scales of the FP16 SIRT residual
+  float *admm_d = nullptr;        // ADMM: 7 volumes (A^T b, u, d, A x, r, p, h)
+  double *admm_dot_d = nullptr;   // ADMM: dot partials + the 3 CG scalars
   bool wt_ready = false, wtvol_ready = false;
   int filt_nx = 0, filt_npad = 0, filt_log2m = 0;
   float2 *ghat_d = nullptr, *tw_d = nullptr;
@@ -116,6 +118,8 @@ void release_problem(tr_ctx *c) {
   scratch_free(c, (void **)&c->res16_d, proj_elems(c) * 2);
   scratch_free(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt);
   scratch_free(c, (void **)&c->rscale_d, sizeof(float) * c->nt);
+  scratch_free(c, (void **)&c->admm_d, 7 * vol_elems(c) * sizeof(float));
+  scratch_free(c, (void **)&c->admm_dot_d, (kAdmmParts + 3) * sizeof(double));
   if (c->geo_d) {
     cudaFree(c->geo_d);
     c->geo_d = nullptr;
@@ -270,6 +274,27 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   c->chunk_bp = chunk_for(kSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
   c->chunk_fp = chunk_for(kSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
   c->wt_ready = c->wtvol_ready = false;
+  return TR_OK;
+}
+
+// Device copies of the host-buffer calls' stack and volume, kept across calls
+// of the same size.
+tr_status host_buffers(tr_ctx *c) {
+  const size_t pn = proj_elems(c), vn = vol_elems(c);
+  if (c->hproj_n != pn) {
+    if (c->hproj_d) cudaFree(c->hproj_d);
+    c->hproj_d = nullptr;
+    c->hproj_n = 0;
+    TR_CUDA(c, cudaMalloc(&c->hproj_d, pn * sizeof(float)));
+    c->hproj_n = pn;
+  }
+  if (c->hvol_n != vn) {
+    if (c->hvol_d) cudaFree(c->hvol_d);
+    c->hvol_d = nullptr;
+    c->hvol_n = 0;
+    TR_CUDA(c, cudaMalloc(&c->hvol_d, vn * sizeof(float)));
+    c->hvol_n = vn;
+  }
   return TR_OK;
 }
 
@@ -697,6 +722,77 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
   return TR_OK;
 }
 
+tr_status tr_admm(tr_ctx *c, const float *proj, float *vol, int outer, int cg_iters, float mu,
+                  float soft, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || outer < 0 || cg_iters < 0)
+    return fail(c, TR_ERR_ARG, "bad ADMM arguments (outer %d, cg %d)", outer, cg_iters);
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t pn = proj_elems(c), V = vol_elems(c);
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection")) ||
+      (st = scratch_alloc(c, (void **)&c->admm_d, 7 * V * sizeof(float), "ADMM volumes")) ||
+      (st = scratch_alloc(c, (void **)&c->admm_dot_d, (kAdmmParts + 3) * sizeof(double),
+                          "ADMM scalars")))
+    return st;
+  if ((st = ensure_wt(c, s))) return st;
+  float *atb = c->admm_d, *u = atb + V, *d = u + V, *ax = d + V, *r = ax + V, *p = r + V,
+        *h = p + V;
+  double *part = c->admm_dot_d, *scal = part + kAdmmParts;
+  const int nsm = c->nsm;
+  // out = (A^T D A + mu I) x, Reproject_admm_atax + ATAmuLTL (main-mpiz.cpp:657-841):
+  // the forward splat, its normalisation by the projection weights, the
+  // unnormalised gather over all tilts, plus mu x.
+  auto apply = [&](const float *x, float *out) -> tr_status {
+    TR_CUDA(c, cudaMemsetAsync(out, 0, V * sizeof(float), s));
+    TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
+    TR_CUDA(c, launch_fp(c->sep, fp_args(c, x, 0, c->th, c->val_d, 0, c->nt), s));
+    TR_CUDA(c, admm_normalize(c->val_d, c->wt_d, pn, nsm, s));
+    TR_CUDA(c, run_bp(c, BP_SUM, bp_args(c, out, 0, c->th, c->val_d, 0, c->nt, 1.f), s));
+    TR_CUDA(c, admm_add_scaled(out, x, mu, V, nsm, s));
+    return TR_OK;
+  };
+  // A^T b (Reproject_admm_htb, :603-656), u = d = 0.
+  TR_CUDA(c, cudaMemsetAsync(atb, 0, 3 * V * sizeof(float), s));
+  TR_CUDA(c, run_bp(c, BP_SUM, bp_args(c, atb, 0, c->th, proj, 0, c->nt, 1.f), s));
+  for (int it = 0; it < outer; ++it) {
+    // The reference adds (u - d) mu to A^T b itself, so the term accumulates
+    // over outer iterations (ATbmuLT on htb, :989).
+    TR_CUDA(c, admm_atb(atb, u, d, mu, V, nsm, s));
+    if ((st = apply(vol, ax))) return st;
+    // applycg (:843-938)
+    TR_CUDA(c, admm_cg_init(r, p, atb, ax, V, nsm, s));
+    for (int k = 0; k < cg_iters; ++k) {
+      if ((st = apply(p, h))) return st;
+      TR_CUDA(c, admm_dot(r, r, V, part, scal + 0, s));
+      TR_CUDA(c, admm_dot(h, p, V, part, scal + 1, s));
+      TR_CUDA(c, admm_x_update(vol, p, scal, V, nsm, s));
+      if ((st = apply(vol, ax))) return st;
+      TR_CUDA(c, admm_r_update(r, atb, ax, V, nsm, s));
+      TR_CUDA(c, admm_dot(r, h, V, part, scal + 2, s));
+      TR_CUDA(c, admm_p_update(p, r, scal, V, nsm, s));
+    }
+    TR_CUDA(c, admm_soft(u, d, vol, soft, V, nsm, s));
+  }
+  return TR_OK;
+}
+
+tr_status tr_admm_host(tr_ctx *c, const float *proj_h, float *vol_h, int outer, int cg_iters,
+                       float mu, float soft) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
+  if ((st = host_buffers(c))) return st;
+  cudaStream_t s = c->io_stream;
+  const size_t pn = proj_elems(c), vn = vol_elems(c);
+  TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice, s));
+  TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));
+  if ((st = tr_admm(c, c->hproj_d, c->hvol_d, outer, cg_iters, mu, soft, s))) return st;
+  TR_CUDA(c, cudaMemcpyAsync(vol_h, c->hvol_d, vn * sizeof(float), cudaMemcpyDeviceToHost, s));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  return take_timeout(c);
+}
+
 tr_status tr_wbp(tr_ctx *c, float *proj, float *vol, void *stream) {
   tr_status st = tr_filter_rweight(c, proj, stream);
   if (st) return st;
@@ -709,20 +805,7 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   if (st) return st;
   if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
   const size_t pn = proj_elems(c), vn = vol_elems(c);
-  if (c->hproj_n != pn) {
-    if (c->hproj_d) cudaFree(c->hproj_d);
-    c->hproj_d = nullptr;
-    c->hproj_n = 0;
-    TR_CUDA(c, cudaMalloc(&c->hproj_d, pn * sizeof(float)));
-    c->hproj_n = pn;
-  }
-  if (c->hvol_n != vn) {
-    if (c->hvol_d) cudaFree(c->hvol_d);
-    c->hvol_d = nullptr;
-    c->hvol_n = 0;
-    TR_CUDA(c, cudaMalloc(&c->hvol_d, vn * sizeof(float)));
-    c->hvol_n = vn;
-  }
+  if ((st = host_buffers(c))) return st;
   cudaStream_t s = c->io_stream;
   TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice, s));
   TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));

@@ -64,6 +64,7 @@ enum BpMode {
   BP_NORM = 0,     // vol += gamma * sum_t s/c      (BPT / WBP / SART update)
   BP_SIRT = 1,     // vol += gamma * (sum_t s) / wtvol where wtvol != 0
   BP_WEIGHTS = 2,  // out = sum_t c                 (SIRT voxel weights)
+  BP_SUM = 3,      // vol += gamma * sum_t s        (unnormalised gather, A^T)
 };
 
 struct BpArgs {
@@ -198,6 +199,26 @@ cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const fl
 cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
 cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int mode,
                               cudaStream_t s);
+
+// ADMM pieces (tr_admm.cu)
+constexpr int kAdmmParts = 592;  // blocks of a deterministic dot product
+cudaError_t admm_normalize(float *val, const float *wt, size_t n, int nsm, cudaStream_t s);
+cudaError_t admm_add_scaled(float *out, const float *x, float mu, size_t n, int nsm,
+                            cudaStream_t s);
+cudaError_t admm_atb(float *atb, const float *u, const float *d, float mu, size_t n, int nsm,
+                     cudaStream_t s);
+cudaError_t admm_cg_init(float *r, float *p, const float *b, const float *a, size_t n, int nsm,
+                         cudaStream_t s);
+cudaError_t admm_dot(const float *a, const float *b, size_t n, double *part, double *out,
+                     cudaStream_t s);
+cudaError_t admm_x_update(float *vol, const float *p, const double *scal, size_t n, int nsm,
+                          cudaStream_t s);
+cudaError_t admm_r_update(float *r, const float *b, const float *ax, size_t n, int nsm,
+                          cudaStream_t s);
+cudaError_t admm_p_update(float *p, const float *r, const double *scal, size_t n, int nsm,
+                          cudaStream_t s);
+cudaError_t admm_soft(float *u, float *d, const float *x, float soft, size_t n, int nsm,
+                      cudaStream_t s);
 dim3 bp_tile_grid(const VolView &v);
 dim3 fp_tile_grid(const VolView &v);
 bool batch_bp_layout(const BpArgs &a0, bool sep, size_t budget, BatchBp *out, size_t *smem);

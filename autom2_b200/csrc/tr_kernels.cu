@@ -289,7 +289,7 @@ __device__ __forceinline__ void bp_epilogue(const BpArgs &a, const float (&acc)[
     const int z = zbase + k;
     if (z >= a.v.nz) break;
     const size_t idx = (size_t)y * a.v.sy + (size_t)z * a.v.sz + x;
-    if (MODE == BP_NORM) {
+    if (MODE == BP_NORM || MODE == BP_SUM) {
       a.v.vol[idx] += a.gamma * acc[k];
     } else if (MODE == BP_SIRT) {
       const float w = a.wtvol[idx];
@@ -1179,6 +1179,9 @@ cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s) {
   if (mode == BP_WEIGHTS)
     return sep ? launch_bp_any<BP_WEIGHTS, true, float>(a, s)
                : launch_bp_any<BP_WEIGHTS, false, float>(a, s);
+  if (mode == BP_SUM)  // FP32 images only
+    return sep ? launch_bp_any<BP_SUM, true, float>(a, s)
+               : launch_bp_any<BP_SUM, false, float>(a, s);
   if (a.img.dtype == IMG_F16) return launch_bp_it<__half>(mode, sep, a, s);
   if (a.img.dtype == IMG_BF16) return launch_bp_it<__nv_bfloat16>(mode, sep, a, s);
   return launch_bp_it<float>(mode, sep, a, s);

@@ -89,6 +89,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_update_geometry.argtypes = [vp, dp, vp]
     lib.tr_filter_rweight.argtypes = [vp, vp, vp]
     lib.tr_filter_fbp.argtypes = [vp, vp, i, vp]
+    lib.tr_admm.argtypes = [vp, vp, vp, i, i, f, f, vp]
+    lib.tr_admm_host.argtypes = [vp, vp, vp, i, i, f, f]
     lib.tr_backproject.argtypes = [vp, vp, vp, i, i, vp]
     lib.tr_forward_project.argtypes = [vp, vp, i, i, vp, vp, vp]
     lib.tr_sirt.argtypes = [vp, vp, vp, i, f, vp]
@@ -255,6 +257,17 @@ class Engine:
     def sart(self, proj, vol, iters, gamma):
         self._check(self.lib.tr_sart(self.h, _ptr(proj), _ptr(vol), iters, gamma,
                                      _stream(self.device)), "tr_sart")
+
+    def admm(self, proj, vol, outer, cg_iters, mu, soft):
+        """ADMM with a soft threshold, in place on vol (see tr_admm)."""
+        self._check(self.lib.tr_admm(self.h, _ptr(proj), _ptr(vol), outer, cg_iters, mu, soft,
+                                     _stream(self.device)), "tr_admm")
+
+    def admm_host(self, proj: np.ndarray, vol: np.ndarray, outer, cg_iters, mu, soft):
+        assert proj.dtype == np.float32 and proj.flags.c_contiguous
+        assert vol.dtype == np.float32 and vol.flags.c_contiguous
+        self._check(self.lib.tr_admm_host(self.h, proj.ctypes.data, vol.ctypes.data, outer,
+                                          cg_iters, mu, soft), "tr_admm_host")
 
     def wbp(self, proj, vol):
         self._check(self.lib.tr_wbp(self.h, _ptr(proj), _ptr(vol), _stream(self.device)),

@@ -174,6 +174,18 @@ tr_status tr_sart_update(tr_ctx *ctx, const float *resid_plane_dev, int tilt,
                          float *vol_dev, int z0, int nz, float gamma,
                          void *stream);
 
+/* ADMM with a soft-threshold (l1) prior, in place on vol_dev (the starting
+ * volume): TiltRecZ's ADMM (main-mpiz.cpp:958-1013, --method
+ * ADMM,outer,cg,mu,soft), with the same algorithm and its quirks kept: A^T b
+ * accumulates the (u - d) mu terms of every outer iteration; each CG
+ * iteration applies (A^T D A + mu I) twice (D = 1/projection weights where
+ * they exceed 1e-5); dot products in FP64.  Any layout. */
+tr_status tr_admm(tr_ctx *ctx, const float *proj_dev, float *vol_dev, int outer,
+                  int cg_iters, float mu, float soft, void *stream);
+/* tr_admm from host buffers (as tr_reconstruct_host). */
+tr_status tr_admm_host(tr_ctx *ctx, const float *proj_host, float *vol_host,
+                       int outer, int cg_iters, float mu, float soft);
+
 /* WBP: filter proj_dev in place, then vol += back-projection.
  * main-mpi.cpp:841-846 (ApplyFilterInplace mode 2 + BackProject), CuFBP with
  * filterMode 2 (recon_y.cuh:28). */

@@ -193,6 +193,9 @@ class Reference:
         y.ref_y_sirt_threaded.restype = C.c_double
         z.ref_z_run.argtypes = [C.c_int] + geo + [_f32p, _f32p, C.c_int, C.c_float, C.c_char_p]
         z.ref_z_run.restype = C.c_int
+        z.ref_z_admm.argtypes = geo + [_f32p, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
+                                       C.c_char_p]
+        z.ref_z_admm.restype = C.c_int
 
     def coeffs20(self, angles, offset=0.0, pitch=0.0, zshift=0.0):
         a = _c(angles, np.float32)
@@ -252,6 +255,19 @@ class Reference:
                                   _c(proj, np.float32), v, iters, gamma, d.encode())
         assert rc == 0, rc
         return v
+
+
+def _ref_z_admm(self, nx, ny, nt, th, c20, origin, proj, vol, outer, cg, mu, soft):
+    """The reference's ADMM (Z layout, vol [th][ny][nx])."""
+    v = _c(vol, np.float32).copy()
+    with tempfile.TemporaryDirectory() as d:
+        rc = self.z.ref_z_admm(nx, ny, nt, th, _c(c20, np.float64), *origin,
+                               _c(proj, np.float32), v, outer, cg, mu, soft, d.encode())
+    assert rc == 0, rc
+    return v
+
+
+Reference.z_admm = _ref_z_admm
 
 
 def rel_l2(a, b) -> float:

@@ -71,6 +71,8 @@ void SART(const Point3DF &origin, MrcStackM &projs, Volume &vol,
           Coeff coeffv[], int iteration, float gamma);
 void SIRT(const Point3DF &origin, MrcStackM &projs, Volume &vol,
           Coeff coeffv[], int iteration, float gamma);
+void ADMM(const Point3DF &origin, MrcStackM &projs, Volume &vol, Coeff coeffv[],
+          int maxOutIter, int numberIteration, float mu, float soft);
 #endif
 
 namespace {
@@ -329,6 +331,31 @@ int ref_z_run(int mode, int nx, int ny, int nt, int th, const double *c20,
       SIRT(o, s, v, c.data(), iters, gamma);
     else if (mode == 4)
       SART(o, s, v, c.data(), iters, gamma);
+    g_deferred = nullptr;
+  }
+  for (void *p : deferred) __real__ZdaPv(p);
+  s.Close();
+  unlink(path.c_str());
+  return 0;
+}
+// ADMM (main-mpiz.cpp:958-1013) on the Z layout, as ref_z_run.
+int ref_z_admm(int nx, int ny, int nt, int th, const double *c20, float ox, float oy,
+               float oz, const float *proj, float *vol, int outer, int cg, float mu,
+               float soft, const char *tmpdir) {
+  std::string path = std::string(tmpdir) + "/oracle_z_stack_" +
+                     std::to_string((long)getpid()) + ".mrc";
+  if (write_stack(path.c_str(), nx, ny, nt, proj)) return -1;
+  std::vector<Coeff> c = to_coeffs(c20, nt);
+  Point3DF o{ox, oy, oz};
+  MrcStackM s;
+  if (!s.ReadFile(path.c_str())) return -2;
+  s.ReadHeader();
+  Volume v(0, 0, 0, ny, nx, th, vol);
+  std::vector<void *> deferred;
+  {
+    QuietStdout q;
+    g_deferred = &deferred;
+    ADMM(o, s, v, c.data(), outer, cg, mu, soft);
     g_deferred = nullptr;
   }
   for (void *p : deferred) __real__ZdaPv(p);

@@ -153,6 +153,19 @@ def test_fbp_vs_oracle(case, restatement, layout):
     assert O.rel_l2(got, restated(layout, proj, ang, geometry, "FBP")) < TOL
 
 
+@pytest.mark.parametrize("method", ["ADMM,1,1,0.5,0.01", "ADMM,2,1,0.5,0.01"])
+def test_tiltrecz_admm_vs_tiltrecz_mpi(case, method):
+    """ADMM through the drop-in executable against TiltRecZ-mpi's (bar 1e-4,
+    as for the ADMM kernels: its CG amplifies float rounding)."""
+    d, proj, ang = case
+    a, b = d / f"oz_{method}.mrc", d / f"rz_{method}.mrc"
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", "0,0,0,10", "--method", method]
+    ours(1, *common, "--output", str(a))
+    reference(1, *common, "--output", str(b))
+    compare(a, b, tol=1e-4)
+
+
 @pytest.mark.parametrize("method,iters", [("BPT", 0), ("SIRT", 2)])
 def test_tiltrecz_vs_oracle(case, restatement, method, iters):
     d, proj, ang = case

@@ -260,3 +260,44 @@ def test_fbp_reconstruction(engine, restatement, layout):
     g = R.geom(nx, ny, nt, th, layout, 0, org)
     want = R.backproject(g, c8, R.filter_fbp(proj, 0), np.zeros(vol0.shape, np.float32))
     assert O.rel_l2(vol, want) < TOL
+
+
+@pytest.mark.parametrize("outer,cg", [(1, 1), (2, 1), (3, 1)])
+def test_admm_vs_reference(engine, restatement, reference, outer, cg):
+    """ADMM against the reference's own ADMM (TiltRecZ-mpi's routine,
+    compiled in oracle/_ref), bar 1e-4.  One CG iteration per outer step: the
+    reference's CG update p = r + beta p takes beta = +(r.Ap)/(p.Ap), the
+    opposite sign of the conjugate direction, so from the second CG iteration
+    on it diverges (on this data cg = 3 reaches 9e10 and a 1e-6 change of
+    the input changes the result by 100 %; cg = 4 gives NaN).  Both sides run
+    that same algorithm; beyond one CG iteration only chaos is compared."""
+    nx, ny, nt, th = 48, 20, 9, 10
+    rng = np.random.default_rng(outer * 10 + cg)
+    ang = np.linspace(-60, 60, nt).astype(np.float32)
+    c8 = restatement.coeffs(ang, 0.5, 0.0, 1.0)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    org = T.default_origin(T.LAYOUT_Z, nx, ny, th)
+    engine.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Z, org)
+    vol = torch.zeros((th, ny, nx), device="cuda")
+    engine.admm(dev(proj), vol, outer, cg, 0.5, 0.01)
+    want = reference.z_admm(nx, ny, nt, th, O.coeff20(c8), org, proj,
+                            np.zeros((th, ny, nx), np.float32), outer, cg, 0.5, 0.01)
+    assert np.isfinite(want).all()
+    assert O.rel_l2(host(vol), want) < 1e-4
+
+
+def test_admm_layouts_agree(engine, restatement):
+    """The same problem in the Y and Z layouts (same origin) gives the same
+    volume, transposed."""
+    nx, ny, nt, th = 40, 16, 7, 12
+    rng = np.random.default_rng(21)
+    c8 = restatement.coeffs(np.linspace(-55, 55, nt).astype(np.float32), 0.0, 2.0, 0.0)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    org = (nx * 0.5, ny * 0.5, th * 0.5)
+    engine.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Z, org)
+    vz = torch.zeros((th, ny, nx), device="cuda")
+    engine.admm(dev(proj), vz, 1, 3, 0.5, 0.01)
+    engine.set_problem(nx, ny, nt, th, c8, T.LAYOUT_Y, org)
+    vy = torch.zeros((ny, th, nx), device="cuda")
+    engine.admm(dev(proj), vy, 1, 3, 0.5, 0.01)
+    assert O.rel_l2(host(vy).transpose(1, 0, 2), host(vz)) < 1e-5
