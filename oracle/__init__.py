@@ -39,8 +39,15 @@ def build(with_reference: bool | None = None) -> None:
     if with_reference is None:
         with_reference = os.path.isdir(REFERENCE_SOURCES)
     if with_reference:
-        subprocess.run(["make", "-s", "ref", f"REF={REFERENCE_SOURCES}"],
+        subprocess.run(["make", "-s", "ref", "refgpu", f"REF={REFERENCE_SOURCES}"],
                        cwd=HERE, check=True)
+
+
+def reference_gpu_executable(layout: int = 0) -> str | None:
+    """The reference's own TiltRec-cuda / TiltRecZ-cuda compiled for sm_100a
+    (``make refgpu``), or None where they were not built."""
+    path = os.path.join(REF_DIR, "TiltRec-cuda" if layout == 0 else "TiltRecZ-cuda")
+    return path if os.path.exists(path) else None
 
 
 class Geom(C.Structure):
