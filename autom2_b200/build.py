@@ -83,6 +83,13 @@ def build_cli(force: bool = False) -> list[str]:
                   "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
             os.replace(out + ".tmp", out)
         outs.append(out)
+    out = os.path.join(BINDIR, "resample")
+    srcs_r = [os.path.join(CLI, "mrc_io.cpp"), os.path.join(CLI, "resample_cli.cpp")]
+    if force or not _newer(out, srcs_r + [os.path.join(CLI, "mrc_io.h"), LIB]):
+        _run(["g++", "-std=c++17", "-O2", "-I", INCLUDE, "-I", CLI, "-o", out + ".tmp", *srcs_r,
+              "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
+        os.replace(out + ".tmp", out)
+    outs.append(out)
     return outs
 
 

@@ -115,6 +115,21 @@ bool write_volume(const std::string &path, const MrcHeader &h, const void *data,
   return true;
 }
 
+bool write_with_extended(const std::string &path, const MrcHeader &h, const float *data,
+                         size_t count, std::string *err) {
+  FILE *f = fopen(path.c_str(), "wb");
+  if (!f) return fail(err, "cannot create " + path);
+  bool ok = fwrite(&h, 1, sizeof(h), f) == sizeof(h);
+  if (ok && h.next > 0) {
+    std::vector<char> zeros((size_t)h.next, 0);
+    ok = fwrite(zeros.data(), 1, zeros.size(), f) == zeros.size();
+  }
+  if (ok) ok = fwrite(data, sizeof(float), count, f) == count;
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(err, "write failed for " + path);
+  return true;
+}
+
 bool read_angles(const std::string &path, std::vector<float> *angles, std::string *err) {
   std::ifstream in(path);
   if (!in.good()) return fail(err, "cannot open tilt file " + path);

@@ -65,6 +65,10 @@ void update_stats(MrcHeader *h, const float *section, size_t n);
 bool write_volume(const std::string &path, const MrcHeader &h, const void *data,
                   size_t bytes, std::string *err);
 
+// Writes header, h.next zero bytes of extended header, then float data.
+bool write_with_extended(const std::string &path, const MrcHeader &h, const float *data,
+                         size_t count, std::string *err);
+
 // Tilt angles: whitespace-separated floats until the first that fails to
 // parse (ReadAngles, main-mpi.cpp:62-83).
 bool read_angles(const std::string &path, std::vector<float> *angles, std::string *err);

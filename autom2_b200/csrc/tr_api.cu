@@ -826,6 +826,44 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   return take_timeout(c);
 }
 
+tr_status tr_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst,
+                          void *stream) {
+  if (!src || !dst || nx < 1 || ny < 1 || nt < 1 || bin < 1 || bin > 64 || nx / bin < 1 ||
+      ny / bin < 1)
+    return TR_ERR_ARG;
+  if (launch_resample_bin(src, nx, ny, nt, bin, dst, (cudaStream_t)stream) != cudaSuccess)
+    return TR_ERR_CUDA;
+  return TR_OK;
+}
+
+tr_status tr_resample_bin_host(int device, const float *src, int nx, int ny, int nt, int bin,
+                               float *dst) {
+  if (!src || !dst || nx < 1 || ny < 1 || nt < 1 || bin < 1 || bin > 64 || nx / bin < 1 ||
+      ny / bin < 1)
+    return TR_ERR_ARG;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return TR_ERR_ARG;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) return TR_ERR_CUDA;
+  const size_t in_b = (size_t)nx * ny * nt * sizeof(float);
+  const size_t out_b = (size_t)(nx / bin) * (ny / bin) * nt * sizeof(float);
+  float *s_d = nullptr, *d_d = nullptr;
+  tr_status st = TR_OK;
+  if (cudaMalloc(&s_d, in_b) != cudaSuccess || cudaMalloc(&d_d, out_b) != cudaSuccess) {
+    cudaGetLastError();
+    st = TR_ERR_OOM;
+  } else if (cudaMemcpy(s_d, src, in_b, cudaMemcpyHostToDevice) != cudaSuccess ||
+             launch_resample_bin(s_d, nx, ny, nt, bin, d_d, nullptr) != cudaSuccess ||
+             cudaMemcpy(dst, d_d, out_b, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    st = TR_ERR_CUDA;
+  }
+  if (s_d) cudaFree(s_d);
+  if (d_d) cudaFree(d_d);
+  return st;
+}
+
 tr_status tr_synchronize(tr_ctx *c) {
   if (!c) return TR_ERR_ARG;
   TR_CUDA(c, cudaSetDevice(c->device));

@@ -182,4 +182,61 @@ cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int m
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ area binning
+//
+// The GUI chain's `resample -b bin` step before TiltRec
+// (resample/src/main/main.cpp:14-58, 67-147) shrinks every image to
+// (nx/bin) x (ny/bin) with OpenCV's area resize: output pixel (i, j) is the
+// mean of the input over [i sx, (i+1) sx) x [j sy, (j+1) sy), sx = nx/(nx/bin),
+// partial pixels weighted by their overlap (an exact block mean when bin
+// divides the size).  One thread per output pixel, separable sums in FP64.
+
+__device__ __forceinline__ int area_axis(int n, int dn, int d, int *first, double *w, int cap) {
+  const double scale = (double)n / dn;
+  const double a = d * scale, b = a + scale > n ? (double)n : a + scale;
+  const int i0 = (int)floor(a), i1 = (int)ceil(b);
+  const double width = b - a;
+  int k = 0;
+  for (int i = i0; i < i1 && k < cap; ++i, ++k) {
+    const double lo = i > a ? i : a, hi = i + 1 < b ? i + 1 : b;
+    w[k] = (hi - lo) / width;
+  }
+  *first = i0;
+  return k;
+}
+
+constexpr int kBinMax = 64;  // largest bin factor (weights per axis: bin + 1)
+
+__global__ void resample_bin_kernel(const float *__restrict__ src, int nx, int ny, int nt,
+                                    int dnx, int dny, float *__restrict__ dst) {
+  const size_t total = (size_t)dnx * dny * nt;
+  for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < total;
+       o += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(o % dnx);
+    const size_t jt = o / dnx;
+    const int j = (int)(jt % dny), t = (int)(jt / dny);
+    double wx[kBinMax + 2], wy[kBinMax + 2];
+    int x0, y0;
+    const int kx = area_axis(nx, dnx, i, &x0, wx, kBinMax + 2);
+    const int ky = area_axis(ny, dny, j, &y0, wy, kBinMax + 2);
+    double acc = 0.0;
+    for (int b = 0; b < ky; ++b) {
+      const float *row = src + ((size_t)t * ny + y0 + b) * nx + x0;
+      double r = 0.0;
+      for (int a = 0; a < kx; ++a) r += wx[a] * (double)row[a];
+      acc += wy[b] * r;
+    }
+    dst[o] = (float)acc;
+  }
+}
+
+cudaError_t launch_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst,
+                                cudaStream_t s) {
+  const int dnx = nx / bin, dny = ny / bin;
+  const size_t total = (size_t)dnx * dny * nt;
+  const unsigned blocks = (unsigned)std::min<size_t>((total + 255) / 256, 148 * 16);
+  resample_bin_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(src, nx, ny, nt, dnx, dny, dst);
+  return cudaGetLastError();
+}
+
 }  // namespace trb

@@ -199,6 +199,8 @@ cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const fl
 cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
 cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int mode,
                               cudaStream_t s);
+cudaError_t launch_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst,
+                                cudaStream_t s);
 
 // ADMM pieces (tr_admm.cu)
 constexpr int kAdmmParts = 592;  // blocks of a deterministic dot product

@@ -449,3 +449,20 @@ class Scheduler:
             self.close()
         except Exception:
             pass
+
+
+def resample_bin(stack, bin_factor: int):
+    """Area binning of a CUDA tensor [nt][ny][nx] by an integer factor
+    (tr_resample_bin); returns a new tensor [nt][ny/bin][nx/bin]."""
+    import torch
+    lib = load_library()
+    lib.tr_resample_bin.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                    C.c_void_p, C.c_void_p]
+    nt, ny, nx = stack.shape
+    out = torch.empty((nt, ny // bin_factor, nx // bin_factor), dtype=torch.float32,
+                      device=stack.device)
+    st = lib.tr_resample_bin(stack.data_ptr(), nx, ny, nt, bin_factor, out.data_ptr(),
+                             _stream(stack.device.index or 0))
+    if st:
+        raise TiltRecError(st, "tr_resample_bin: " + lib.tr_status_string(st).decode())
+    return out

@@ -314,6 +314,16 @@ tr_status tr_sirt_static(int device, int nx, int ny, int ntilt, int thickness,
                          int iters, float gamma, void *stream);
 size_t tr_static_scratch_limit(void);
 
+/* Area binning of nt images [nt][ny][nx] to [nt][ny/bin][nx/bin] (bin 1..64),
+ * the GUI chain's `resample -b bin` before TiltRec (resample/src/main/
+ * main.cpp:14-58, OpenCV's area resize): each output pixel is the overlap-
+ * weighted mean of its input cell.  Needs no context; runs on the current
+ * device (tr_resample_bin) or copies host buffers through `device`. */
+tr_status tr_resample_bin(const float *src_dev, int nx, int ny, int nt, int bin,
+                          float *dst_dev, void *stream);
+tr_status tr_resample_bin_host(int device, const float *src_host, int nx, int ny,
+                               int nt, int bin, float *dst_host);
+
 /* Wait for all work the context issued. */
 tr_status tr_synchronize(tr_ctx *ctx);
 

@@ -75,6 +75,7 @@ class Restatement:
         lib.orc_filter_rweight.argtypes = [C.c_int, C.c_long, _f32p]
         lib.orc_filter_fbp.argtypes = [C.c_int, C.c_int, C.c_long, _f32p]
         lib.orc_optimal_dft_size.argtypes = [C.c_int]
+        lib.orc_resample_bin.argtypes = [_f32p, C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
         for pfx, p in (("orc_", _f32p), ("orc64_", _f64p)):
             real = C.c_float if pfx == "orc_" else C.c_double
             g = C.POINTER(Geom)
@@ -108,6 +109,14 @@ class Restatement:
         nx = p.shape[-1]
         self.lib.orc_filter_fbp(mode, nx, p.size // nx, p)
         return p
+
+    def resample_bin(self, stack, bin_factor):
+        """Area binning of [nt][ny][nx] by an integer factor."""
+        p = _c(stack, np.float32)
+        nt, ny, nx = p.shape
+        out = np.zeros((nt, ny // bin_factor, nx // bin_factor), np.float32)
+        self.lib.orc_resample_bin(p, nx, ny, nt, bin_factor, out)
+        return out
 
     def optimal_dft_size(self, n):
         return int(self.lib.orc_optimal_dft_size(n))

@@ -198,3 +198,44 @@ int orc_filter_fbp(int mode, int nx, long nrows, float *rows) {
   }
   return L;
 }
+
+/* Overlap weights of one axis: output cell d covers [d*scale, (d+1)*scale)
+ * of n input pixels; w[k] is the covered part of input pixel first + k,
+ * divided by the cell width (clipped at the image end). */
+static int orc_area_axis(int n, int dn, int d, int *first, double *w) {
+  const double scale = (double)n / dn;
+  const double a = d * scale, b = a + scale > n ? (double)n : a + scale;
+  const int i0 = (int)floor(a), i1 = (int)ceil(b);
+  const double width = b - a;
+  int k = 0;
+  for (int i = i0; i < i1; ++i, ++k) {
+    const double lo = i > a ? i : a, hi = i + 1 < b ? i + 1 : b;
+    w[k] = (hi - lo) / width;
+  }
+  *first = i0;
+  return k;
+}
+
+void orc_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst) {
+  const int dnx = nx / bin, dny = ny / bin;
+  double *wx = (double *)malloc(sizeof(double) * (bin + 2));
+  double *wy = (double *)malloc(sizeof(double) * (bin + 2));
+  for (int t = 0; t < nt; ++t)
+    for (int j = 0; j < dny; ++j) {
+      int y0, x0;
+      const int ky = orc_area_axis(ny, dny, j, &y0, wy);
+      for (int i = 0; i < dnx; ++i) {
+        const int kx = orc_area_axis(nx, dnx, i, &x0, wx);
+        double acc = 0;
+        for (int b = 0; b < ky; ++b) {
+          const float *row = src + ((size_t)t * ny + y0 + b) * nx + x0;
+          double r = 0;
+          for (int a = 0; a < kx; ++a) r += wx[a] * (double)row[a];
+          acc += wy[b] * r;
+        }
+        dst[((size_t)t * dny + j) * dnx + i] = (float)acc;
+      }
+    }
+  free(wx);
+  free(wy);
+}

@@ -49,6 +49,14 @@ void orc_filter_rweight(int nx, long nrows, float *rows);
  * L the reference would use. */
 int orc_filter_fbp(int mode, int nx, long nrows, float *rows);
 
+/* Area binning of nt images of nx*ny floats by an integer factor (the GUI
+ * chain's `resample -b bin`, resample/src/main/main.cpp:14-58, 67-147, which
+ * calls OpenCV's area resize to (nx/bin) x (ny/bin)): output pixel (i, j)
+ * is the mean of the input over [i*sx, (i+1)*sx) x [j*sy, (j+1)*sy) with
+ * sx = nx/(nx/bin), sy likewise, partial pixels weighted by their overlap;
+ * separable, in double.  Out: nt * (nx/bin) * (ny/bin). */
+void orc_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst);
+
 /* Smallest integer >= n whose only prime factors are 2, 3 and 5 (the
  * sizes OpenCV's getOptimalDFTSize returns). */
 int orc_optimal_dft_size(int n);

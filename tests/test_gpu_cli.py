@@ -222,3 +222,37 @@ def test_f2b_bytes(case):
         z = np.clip((c[:n4] - gm) / gs, -10, 10)
         want[s0:s0 + n4] = (((z + 10) / 20) * 255).astype(np.uint8)
     assert np.mean(np.abs(got.reshape(-1).astype(int) - want.astype(int)) <= 1) > 0.999
+
+
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_resample_executable(case, restatement, tmp_path, mode):
+    """The resample drop-in: bytes read unsigned and divided by 255, shorts
+    as their value; float output; header the input's with the new sizes."""
+    d, proj, ang = case
+    rng = np.random.default_rng(mode)
+    if mode == 2:
+        data = proj
+    elif mode == 1:
+        data = np.round(proj * 300).astype(np.float32)
+    else:
+        data = rng.integers(0, 256, size=proj.shape).astype(np.float32)
+    src = tmp_path / f"in{mode}.mrc"
+    stored = data.astype(np.uint8).view(np.int8) if mode == 0 else data
+    write_mrc(src, stored, mode=mode, next_bytes=32 if mode == 1 else 0)
+    with open(src, "r+b") as f:  # input statistics the output must carry over
+        f.seek(76)
+        f.write(np.array([-1.5, 2.5, 0.25], "<f4").tobytes())
+    out = tmp_path / f"out{mode}.mrc"
+    exe = os.path.join(BIN, "resample")
+    r = subprocess.run([exe, "-i", str(src), "-o", str(out), "-b", "3"], capture_output=True,
+                       text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    hi, _, _ = read_mrc(src)
+    ho, _, got = read_mrc(out)
+    want = restatement.resample_bin(data / 255.0 if mode == 0 else data, 3)
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 1e-6 * max(1.0, np.abs(want).max())
+    assert int(ho["mode"]) == 2
+    assert [int(v) for v in ho["m"]] == [want.shape[2], want.shape[1], want.shape[0]]
+    for f in ("amin", "amax", "amean", "next"):
+        assert np.array_equal(ho[f], hi[f]), f

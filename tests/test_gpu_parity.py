@@ -301,3 +301,15 @@ def test_admm_layouts_agree(engine, restatement):
     vy = torch.zeros((ny, th, nx), device="cuda")
     engine.admm(dev(proj), vy, 1, 3, 0.5, 0.01)
     assert O.rel_l2(host(vy).transpose(1, 0, 2), host(vz)) < 1e-5
+
+
+@pytest.mark.parametrize("shape,factor", [((3, 64, 96), 2), ((2, 37, 53), 3),
+                                          ((1, 1000, 1023), 4), ((2, 40, 40), 1)])
+def test_resample_bin(engine, restatement, shape, factor):
+    """Device area binning (the resample step) against the oracle."""
+    rng = np.random.default_rng(sum(shape) + factor)
+    a = rng.normal(size=shape).astype(np.float32)
+    got = host(T.resample_bin(dev(a), factor))
+    want = restatement.resample_bin(a, factor)
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 1e-6 * max(1.0, np.abs(want).max())

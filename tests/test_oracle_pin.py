@@ -193,3 +193,18 @@ def test_fbp_filter_restatement_matches_dft_steps(restatement, mode, nx):
         want, L = _fbp_by_dft(rows[r].astype(np.float64), _taps(mode))
         assert L == restatement.optimal_dft_size(nx + 2 + 250)
         assert np.abs(got[r] - want).max() <= 1e-5 * np.abs(want).max()
+
+
+def test_resample_bin_restatement(restatement):
+    """Area binning: a block mean when the factor divides the size; with a
+    remainder the cells still tile the image, so the means agree."""
+    rng = np.random.default_rng(4)
+    a = rng.normal(size=(2, 12, 18)).astype(np.float32)
+    got = restatement.resample_bin(a, 3)
+    want = a.reshape(2, 4, 3, 6, 3).astype(np.float64).mean(axis=(2, 4))
+    assert np.abs(got - want).max() < 1e-6
+    b = rng.normal(size=(1, 13, 17)).astype(np.float32)
+    for f in (2, 3, 5):
+        g = restatement.resample_bin(b, f)
+        assert g.shape == (1, 13 // f, 17 // f)
+        assert abs(g.mean() - b.astype(np.float64).mean()) < 1e-6
