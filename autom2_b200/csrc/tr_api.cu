@@ -864,6 +864,18 @@ tr_status tr_resample_bin_host(int device, const float *src, int nx, int ny, int
   return st;
 }
 
+tr_status tr_selftest_wait(tr_ctx *c, int budget_us) {
+  if (!c || budget_us < 1 || budget_us > 10000000) return TR_ERR_ARG;
+  TR_CUDA(c, cudaSetDevice(c->device));
+  int khz = 0;
+  TR_CUDA(c, cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, c->device));
+  const long long cycles = (long long)khz * budget_us / 1000;
+  TR_CUDA(c, cudaMemsetAsync(c->err_d, 0, 2 * sizeof(int), c->io_stream));
+  TR_CUDA(c, launch_bounded_wait_selftest(cycles, c->err_d, c->io_stream));
+  TR_CUDA(c, cudaStreamSynchronize(c->io_stream));
+  return take_timeout(c);
+}
+
 tr_status tr_synchronize(tr_ctx *c) {
   if (!c) return TR_ERR_ARG;
   TR_CUDA(c, cudaSetDevice(c->device));

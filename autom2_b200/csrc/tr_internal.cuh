@@ -197,6 +197,7 @@ cudaError_t launch_resid_lp(const void *p, int pdtype, const float *ps, const fl
                             const float *wt, size_t plane, int nt, int rdtype, void *r,
                             const float *rs, int nsm, cudaStream_t s);
 cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s);
+cudaError_t launch_bounded_wait_selftest(long long budget, int *err, cudaStream_t s);
 cudaError_t launch_fbp_filter(float *rows, long long nrows, int nx, int L, int mode,
                               cudaStream_t s);
 cudaError_t launch_resample_bin(const float *src, int nx, int ny, int nt, int bin, float *dst,

@@ -869,6 +869,25 @@ __global__ void resid_lp_kernel(const PT *__restrict__ p, const float *__restric
   }
 }
 
+// Self-test of the bounded device wait: one CTA waits on an mbarrier that
+// nothing arrives at, with the budget given; the wait must give up and the
+// CTA report through err[1], as a back-projection whose copies never land.
+__global__ void bounded_wait_selftest_kernel(long long budget, int *err) {
+  __shared__ __align__(8) unsigned long long m;
+  if (threadIdx.x == 0) {
+    mbar_init(&m, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&m, 0u, budget, nullptr);
+  if (!__syncthreads_or(ok) && threadIdx.x == 0) atomicExch(err + 1, 1);
+}
+
+cudaError_t launch_bounded_wait_selftest(long long budget, int *err, cudaStream_t s) {
+  bounded_wait_selftest_kernel<<<1, 32, 0, s>>>(budget, err);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------- batches
 //
 // One batch step: zero the accumulators of the step's forward projections

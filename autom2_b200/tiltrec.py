@@ -105,6 +105,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_backproject_lp.argtypes = [vp, vp, i, vp, vp, i, i, vp]
     lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
     lib.tr_synchronize.argtypes = [vp]
+    lib.tr_selftest_wait.argtypes = [vp, i]
     for name in ("tr_create", "tr_destroy", "tr_set_problem", "tr_update_geometry",
                  "tr_filter_rweight",
                  "tr_backproject", "tr_forward_project", "tr_sirt", "tr_sart",
@@ -308,6 +309,11 @@ class Engine:
 
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")
+
+    def selftest_wait(self, budget_us: int) -> int:
+        """tr_selftest_wait's status (TR_ERR_TIMEOUT = -5 when the bounded
+        wait gave up, as it should)."""
+        return int(self.lib.tr_selftest_wait(self.h, budget_us))
 
 
 def sirt_static(proj, vol, coeff8, iters, gamma, layout=LAYOUT_Y, origin=None,

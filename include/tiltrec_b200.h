@@ -324,6 +324,13 @@ tr_status tr_resample_bin(const float *src_dev, int nx, int ny, int nt, int bin,
 tr_status tr_resample_bin_host(int device, const float *src_host, int nx, int ny,
                                int nt, int bin, float *dst_host);
 
+/* Self-test of the device-side wait limit (no counterpart in the reference):
+ * one CTA waits on a barrier nothing completes, with a budget of budget_us
+ * microseconds of GPU clock.  Returns TR_ERR_TIMEOUT when the wait gave up and
+ * reported as a back-projection does (the expected outcome), after which the
+ * context stays usable. */
+tr_status tr_selftest_wait(tr_ctx *ctx, int budget_us);
+
 /* Wait for all work the context issued. */
 tr_status tr_synchronize(tr_ctx *ctx);
 
