@@ -396,6 +396,8 @@ def run_kernels(args):
     build.build_lib()
     cfg = synth.config("cfg1", args.scale)
     coeff = synth.coefficients(cfg)
+    if args.separable:  # ideal single-axis geometry: the separable kernels
+        coeff = T.geometry_from_angles(cfg.angles)
     nx, ny, nt, th = cfg.nx, cfg.ny, cfg.ntilt, cfg.thickness
     eng = T.Engine(0)
     eng.set_problem(nx, ny, nt, th, coeff, T.LAYOUT_Y)
@@ -409,7 +411,8 @@ def run_kernels(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(1, args.iters)
-    print(json.dumps({"case": f"cfg1/{args.scale}", "proj": [nt, ny, nx],
+    print(json.dumps({"case": f"cfg1/{args.scale}" + (" separable" if args.separable else ""),
+                      "proj": [nt, ny, nx],
                       "volume": [nx, ny, th], "iters": args.iters,
                       "ms_per_iter": ms}), flush=True)
     eng.close()
@@ -801,6 +804,8 @@ def main():
                     help="profiling case only (see run_kernels)")
     ap.add_argument("--scale", type=int, default=2)
     ap.add_argument("--iters", type=int, default=2)
+    ap.add_argument("--separable", action="store_true",
+                    help="profiling case: ideal single-axis geometry")
     ap.add_argument("--workload", default="sirt",
                     choices=["sirt", "cfg0", "cfg2", "batch", "serve"],
                     help="sirt: the headline SIRT-30 line; batch / serve: the batched "
