@@ -425,11 +425,59 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// Five consecutive raw window elements p[0..4] as floats; p is 16-byte aligned
+// for 32-bit elements and 8-byte aligned for 16-bit ones.
+__device__ __forceinline__ float bits16_to_f(unsigned b, const __half *) {
+  return __half2float(__ushort_as_half((unsigned short)b));
+}
+__device__ __forceinline__ float bits16_to_f(unsigned b, const __nv_bfloat16 *) {
+  return __bfloat162float(__ushort_as_bfloat16((unsigned short)b));
+}
+template <typename IT>
+__device__ __forceinline__ void load5(const IT *p, float (&v)[5]) {
+  if constexpr (std::is_same<IT, float>::value) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    v[0] = a.x;
+    v[1] = a.y;
+    v[2] = a.z;
+    v[3] = a.w;
+  } else {
+    const uint2 a = *reinterpret_cast<const uint2 *>(p);
+    v[0] = bits16_to_f(a.x & 0xFFFFu, p);
+    v[1] = bits16_to_f(a.x >> 16, p);
+    v[2] = bits16_to_f(a.y & 0xFFFFu, p);
+    v[3] = bits16_to_f(a.y >> 16, p);
+  }
+  v[4] = to_f(p[4]);
+}
+
+// Writes the four table entries (b - s, s), s = n - b, of a group from the
+// values b_m = p[m], n_m = p[m+1] (32-byte aligned destination).
+__device__ __forceinline__ void store_group(float2 *dst, const float (&p)[5]) {
+  float e[8];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const float sl = p[m + 1] - p[m];
+    e[2 * m] = p[m] - sl;
+    e[2 * m + 1] = sl;
+  }
+  float4 *d = reinterpret_cast<float4 *>(dst);
+  d[0] = make_float4(e[0], e[1], e[2], e[3]);
+  d[1] = make_float4(e[4], e[5], e[6], e[7]);
+}
+
 // One volume tile (bx, by, bz) of a TMA-staged back-projection.  dsm is the
 // CTA's dynamic shared memory laid out by the launcher, mbar its two
 // initialised mbarriers, and uses[b] the completed phases of mbarrier b so far
 // (a persistent CTA runs many tiles on the same mbarriers).  Returns false
 // when a bounded wait ran out (err words set; the tile's voxels untouched).
+//
+// The tables are staged in groups of four entries per thread: a tilt's window
+// starts at the raw window's first column (the tile's lowest reachable column
+// rounded down to the 16-byte TMA granularity), so a group's five image values
+// come from one aligned vector read and one scalar read of the raw window.
+// Groups touching the image border in normalised mode take the per-entry
+// clamping path; both paths give the same entries as per-entry staging.
 template <int MODE, bool SEP, typename IT>
 __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *tmap, int bx,
                                             int by, int bz, unsigned char *dsm,
@@ -461,6 +509,11 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
       for (int r = 1; r < kTY; ++r) y0 = min(y0, sw[i][r].y0);
       tt[i].jmin = y0;
     }
+    // Table column 0 = raw column 0 = the aligned TMA x coordinate.
+    const int xs = tt[i].kmin & ~(kXAlign - 1), o = tt[i].kmin - xs;
+    tt[i].U0 += (long long)o << 32;
+    tt[i].nq += o;
+    tt[i].kmin = xs;
   }
   __syncthreads();
 
@@ -471,8 +524,8 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
     mbar_expect_tx(&mbar[buf], (unsigned)(nc * bw * bh * (int)sizeof(IT)));
     IT *dst = raw0 + (size_t)buf * chunk * rs;
     for (int i = 0; i < nc; ++i)
-      tma_load_3d(dst + (size_t)i * rs, tmap, tt[c0 + i].kmin & ~(kXAlign - 1),
-                  tt[c0 + i].jmin, a.t0 + c0 + i, &mbar[buf]);
+      tma_load_3d(dst + (size_t)i * rs, tmap, tt[c0 + i].kmin, tt[c0 + i].jmin, a.t0 + c0 + i,
+                  &mbar[buf]);
   };
   if (tid == 0) {
     issue(0, 0);
@@ -504,50 +557,75 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
       return false;
     }
     const IT *R0 = raw0 + (size_t)buf * chunk * rs;
-    EntryWalk w(tid, fh, fw);
-    for (int e = tid; e < nc * per; e += kThreads, w.next(fh, fw)) {
-      const int i = w.i, r = w.r, q = w.q;
+    const int ng = fw >> 2;  // four-entry groups per table row
+    EntryWalk w(tid, fh, ng);
+    for (int g = tid; g < nc * fh * ng; g += kThreads, w.next(fh, ng)) {
+      const int i = w.i, r = w.r, q = w.q << 2;  // q: the group's first column
       const TileTilt &t = tt[c0 + i];
       if (r >= t.nr || q >= t.nq) continue;
-      const IT *R = R0 + (size_t)i * rs;
+      const IT *R = R0 + (size_t)i * rs;  // raw column = table column
       const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
-      const int xs = t.kmin & ~(kXAlign - 1), ys = t.jmin;
-      const int x0 = t.kmin + q;
+      const int xs = t.kmin, ys = t.jmin;
+      const int x0 = xs + q;  // image column of the group's first entry
+      float p[5];
       if (SEP) {
         const SepW s = sw[c0 + i][r];
-        const IT *r0 = R + (s.y0 - ys) * bw - xs, *r1 = r0 + bw;
-        float b = 0.f, n = 0.f;
-        if (MODE == BP_NORM) {
-          if ((s.w0 + s.w1) != 0.f && x0 >= -1 && x0 <= pnx - 1) {
-            const int kb = clampi(x0, 0, pnx - 1), kn = clampi(x0 + 1, 0, pnx - 1);
-            const float c = s.w0 + s.w1;
-            const float w0 = s.w0 * sc, w1 = s.w1 * sc;
-            b = (w0 * (s.w0 != 0.f ? to_f(r0[kb]) : 0.f) + w1 * (s.w1 != 0.f ? to_f(r1[kb]) : 0.f)) / c;
-            n = (w0 * (s.w0 != 0.f ? to_f(r0[kn]) : 0.f) + w1 * (s.w1 != 0.f ? to_f(r1[kn]) : 0.f)) / c;
+        const IT *r0 = R + (s.y0 - ys) * bw, *r1 = r0 + bw;
+        const float w0 = s.w0 * sc, w1 = s.w1 * sc;
+        if (MODE != BP_NORM) {
+          float p0[5], p1[5];
+          load5(r0 + q, p0);
+          load5(r1 + q, p1);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) p[m] = w0 * p0[m] + w1 * p1[m];
+          store_group(tbl2 + (size_t)g * 4, p);
+        } else if ((s.w0 + s.w1) != 0.f && x0 >= 0 && x0 + 4 <= pnx - 1) {
+          const float c = s.w0 + s.w1;
+          float p0[5], p1[5];
+          load5(r0 + q, p0);
+          load5(r1 + q, p1);
+#pragma unroll
+          for (int m = 0; m < 5; ++m)
+            p[m] = (w0 * (s.w0 != 0.f ? p0[m] : 0.f) + w1 * (s.w1 != 0.f ? p1[m] : 0.f)) / c;
+          store_group(tbl2 + (size_t)g * 4, p);
+        } else {  // border: per entry, clamped; zero outside the valid range
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int x = x0 + m;
+            float b = 0.f, n = 0.f;
+            if ((s.w0 + s.w1) != 0.f && x >= -1 && x <= pnx - 1) {
+              const int kb = clampi(x, 0, pnx - 1) - xs, kn = clampi(x + 1, 0, pnx - 1) - xs;
+              const float c = s.w0 + s.w1;
+              b = (w0 * (s.w0 != 0.f ? to_f(r0[kb]) : 0.f) +
+                   w1 * (s.w1 != 0.f ? to_f(r1[kb]) : 0.f)) / c;
+              n = (w0 * (s.w0 != 0.f ? to_f(r0[kn]) : 0.f) +
+                   w1 * (s.w1 != 0.f ? to_f(r1[kn]) : 0.f)) / c;
+            }
+            const float sl = n - b;
+            tbl2[(size_t)g * 4 + m] = make_float2(b - sl, sl);
           }
-        } else {
-          const float w0 = s.w0 * sc, w1 = s.w1 * sc;
-          b = w0 * to_f(r0[x0]) + w1 * to_f(r1[x0]);
-          n = w0 * to_f(r0[x0 + 1]) + w1 * to_f(r1[x0 + 1]);
         }
-        const float sl = n - b;
-        tbl2[e] = make_float2(b - sl, sl);
       } else {
         const int j = ys + r;
-        float b = 0.f, n = 0.f;
-        if (MODE == BP_NORM) {
-          if (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny) {
-            const IT *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
-            b = to_f(row[clampi(x0, 0, pnx - 1)]) * sc;
-            n = to_f(row[clampi(x0 + 1, 0, pnx - 1)]) * sc;
+        if (MODE != BP_NORM || (x0 >= 0 && x0 + 4 <= pnx - 1 && j >= 0 && j <= pny - 1)) {
+          load5(R + r * bw + q, p);
+#pragma unroll
+          for (int m = 0; m < 5; ++m) p[m] *= sc;
+          store_group(tbl2 + (size_t)g * 4, p);
+        } else {  // border: per entry, clamped; zero outside the valid range
+          const IT *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
+#pragma unroll
+          for (int m = 0; m < 4; ++m) {
+            const int x = x0 + m;
+            float b = 0.f, n = 0.f;
+            if (x >= -1 && x <= pnx - 1 && j >= -1 && j <= pny) {
+              b = to_f(row[clampi(x, 0, pnx - 1)]) * sc;
+              n = to_f(row[clampi(x + 1, 0, pnx - 1)]) * sc;
+            }
+            const float sl = n - b;
+            tbl2[(size_t)g * 4 + m] = make_float2(b - sl, sl);
           }
-        } else {
-          const IT *row = R + r * bw - xs;
-          b = to_f(row[x0]) * sc;
-          n = to_f(row[x0 + 1]) * sc;
         }
-        const float sl = n - b;
-        tbl2[e] = make_float2(b - sl, sl);
       }
     }
     __syncthreads();
@@ -1128,13 +1206,17 @@ static bool tma_layout(const BpArgs &a0, bool sep, size_t budget, BpArgs *out,
       (reinterpret_cast<uintptr_t>(im.p) & 15) != 0)
     return false;
   const int fh = sep ? kTY : a0.fh;
-  const int bw = (a0.fw + xal + xal - 1) / xal * xal;
+  // Table rows start at the aligned raw column: up to xal - 1 extra columns,
+  // rounded up to whole four-entry groups; the raw window holds one more
+  // column for the last group's slopes.
+  const int fwt = (a0.fw + xal - 1 + 3) & ~3;
+  const int bw = (fwt + 1 + xal - 1) / xal * xal;
   const int bh = sep ? kTY + 3 : fh + 1;
   if (bw > 256 || bh > 256) return false;
   const int rs = ((bw * bh * es + 127) & ~127) / es;  // elements; 128-byte aligned slots
   const size_t fixed =
       ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
-  const size_t per_tilt = 2 * (size_t)rs * es + (size_t)fh * a0.fw * sizeof(float2);
+  const size_t per_tilt = 2 * (size_t)rs * es + (size_t)fh * fwt * sizeof(float2);
   if (fixed + per_tilt > budget + 64 * 1024) return false;
   int chunk = (int)std::max<size_t>(1, (budget > fixed ? budget - fixed : 0) / per_tilt);
   chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
@@ -1150,6 +1232,7 @@ static bool tma_layout(const BpArgs &a0, bool sep, size_t budget, BpArgs *out,
           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   *out = a0;
+  out->fw = fwt;
   out->chunk = chunk;
   out->tma_bw = bw;
   out->tma_bh = bh;
