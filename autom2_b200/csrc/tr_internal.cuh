@@ -106,6 +106,17 @@ struct TileTilt {
   int nq, nr;        // columns / rows of the window this tile can reach
 };
 
+// Back-projection coordinate starts of one staged tilt: the per-voxel steps
+// and, per warp w (wy = w % kTY, wz = w / kTY), the Q32.32 coordinates of the
+// warp's lane-0 first voxel, U0 + wy A1 + wz kNV A2 (V likewise), so that a
+// thread's start is one 64-bit multiply-add, W + lane A0.
+struct WarpStarts {
+  long long A0, B0;
+  unsigned du, dv;   // Q9.23 steps along z
+  int jmin, check_rows;
+  long long Wu[kThreads / 32], Wv[kThreads / 32];
+};
+
 // Separable rows (b1 = b3 = 0, b2 = 1): per voxel row of the tile, the lower
 // detector row and its weight, as the reference computes them.
 struct SepRow {

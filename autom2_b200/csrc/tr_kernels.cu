@@ -210,12 +210,33 @@ __device__ __forceinline__ float one_plus_frac23(unsigned u) {
   return __uint_as_float(0x3F800000u | (u & 0x7FFFFFu));
 }
 
+// Threads tid < nc * (kThreads / 32) fill ws[0..nc) from the chunk's tile
+// bookkeeping tt[0..nc) and geometry geo[0..nc).
+__device__ __forceinline__ void fill_warp_starts(WarpStarts *ws, const TileTilt *tt,
+                                                 const TiltGeo *geo, int nc, int tid) {
+  constexpr int kW = kThreads / 32;
+  if (tid >= nc * kW) return;
+  const int i = tid / kW, w = tid % kW;
+  const int wy = w % kTY, wz = w / kTY;
+  const TiltGeo &g = geo[i];
+  ws[i].Wu[w] = tt[i].U0 + wy * g.A[1] + (long long)(wz * kNV) * g.A[2];
+  ws[i].Wv[w] = tt[i].V0 + wy * g.B[1] + (long long)(wz * kNV) * g.B[2];
+  if (w == 0) {
+    ws[i].A0 = g.A[0];
+    ws[i].B0 = g.B[0];
+    ws[i].du = q23_step(g.A[2]);
+    ws[i].dv = q23_step(g.B[2]);
+    ws[i].jmin = tt[i].jmin;
+    ws[i].check_rows = tt[i].check_rows;
+  }
+}
+
 template <int MODE, bool SEP, bool KAHAN>
 __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kNV],
-                                              const void *tblv,
-                                              const TileTilt *tt, const TiltGeo *geo,
+                                              const void *tblv, const WarpStarts *ws,
                                               int nc, int per, int fw, int pny,
                                               int lane, int wy, int wz) {
+  const int w = wz * kTY + wy;  // the warp's index in the CTA
   // KAHAN: the chunk's tilts (at most kMaxChunk) sum into a plain partial,
   // which joins the voxel's total by one compensated addition per chunk.
   float part[kNV];
@@ -225,11 +246,9 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
     for (int k = 0; k < kNV; ++k) part[k] = 0.f;
   }
   for (int i = 0; i < nc; ++i) {
-    const TiltGeo &g = geo[i];
-    const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
-    unsigned u = q23((unsigned long long)(tt[i].U0 + lane * A0 + wy * A1 +
-                                          (long long)(wz * kNV) * A2));
-    const unsigned du = q23_step(A2);
+    const WarpStarts &st = ws[i];
+    unsigned u = q23((unsigned long long)(st.Wu[w] + lane * st.A0));
+    const unsigned du = st.du;
     if (SEP) {
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)(i * kTY + wy) * fw;
 #pragma unroll
@@ -239,13 +258,11 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
         u += du;
       }
     } else {
-      const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
-      unsigned v = q23((unsigned long long)(tt[i].V0 + lane * B0 + wy * B1 +
-                                            (long long)(wz * kNV) * B2));
-      const unsigned dv = q23_step(B2);
+      unsigned v = q23((unsigned long long)(st.Wv[w] + lane * st.B0));
+      const unsigned dv = st.dv;
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)i * per;
-      const int jmin = tt[i].jmin;
-      if (MODE == BP_NORM && tt[i].check_rows) {
+      const int jmin = st.jmin;
+      if (MODE == BP_NORM && st.check_rows) {
 #pragma unroll
         for (int k = 0; k < kNV; ++k) {
           const int q = (int)(u >> 23), r = (int)(v >> 23);
@@ -310,6 +327,7 @@ __global__ void __launch_bounds__(kThreads)
   float2 *tbl2 = reinterpret_cast<float2 *>(tbl_raw);
   __shared__ TileTilt tt[kMaxChunk];
   __shared__ SepW sw[kMaxChunk][kTY];
+  __shared__ WarpStarts ws[kMaxChunk];
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -330,6 +348,7 @@ __global__ void __launch_bounds__(kThreads)
       tile_setup(a.geo[a.t0 + c0 + tid], xc, yc, zc, a.ox, a.oy, a.oz, pny, SEP,
                  kTX - 1, kTY - 1, kTZ - 1, tt[tid], sw[tid]);
     __syncthreads();
+    fill_warp_starts(ws, tt, a.geo + a.t0 + c0, nc, tid);
     // Stage the interpolation tables of the chunk.  One flat loop over the
     // chunk's entries keeps many independent image loads in flight per
     // thread; entries outside a tilt's reachable window are skipped.
@@ -362,8 +381,7 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
     __syncthreads();
-    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tbl_raw, tt, a.geo + a.t0 + c0, nc, per, fw,
-                                    pny, lane, wy, wz);
+    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tbl_raw, ws, nc, per, fw, pny, lane, wy, wz);
     __syncthreads();
   }
   bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
@@ -498,6 +516,7 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
   SepW(*sw)[kTY] = reinterpret_cast<SepW(*)[kTY]>(dsm + (size_t)nt * sizeof(TileTilt));
   IT *raw0 = reinterpret_cast<IT *>(dsm + a.tma_raw_offset);
   float *tblf = reinterpret_cast<float *>(raw0 + 2 * (size_t)chunk * rs);  // float2 entries
+  WarpStarts *ws = reinterpret_cast<WarpStarts *>(tblf + 2 * (size_t)chunk * per);
   constexpr int kXAlign = 16 / (int)sizeof(IT);  // TMA x coordinates: 16-byte multiples
   float2 *tbl2 = reinterpret_cast<float2 *>(tblf);
 
@@ -556,6 +575,7 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
                           1ll << 28, nullptr);
       return false;
     }
+    fill_warp_starts(ws, tt + c0, a.geo + a.t0 + c0, nc, tid);
     const IT *R0 = raw0 + (size_t)buf * chunk * rs;
     const int ng = fw >> 2;  // four-entry groups per table row
     EntryWalk w(tid, fh, ng);
@@ -630,8 +650,7 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
     }
     __syncthreads();
     if (tid == 0 && c + 2 < nchunks) issue(c + 2, buf);
-    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tblf, tt + c0, a.geo + a.t0 + c0, nc, per, fw,
-                                    pny, lane, wy, wz);
+    bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tblf, ws, nc, per, fw, pny, lane, wy, wz);
     __syncthreads();
   }
   uses[0] += (unsigned)(nchunks + 1) / 2;
@@ -1216,7 +1235,8 @@ static bool tma_layout(const BpArgs &a0, bool sep, size_t budget, BpArgs *out,
   const int rs = ((bw * bh * es + 127) & ~127) / es;  // elements; 128-byte aligned slots
   const size_t fixed =
       ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
-  const size_t per_tilt = 2 * (size_t)rs * es + (size_t)fh * fwt * sizeof(float2);
+  const size_t per_tilt =
+      2 * (size_t)rs * es + (size_t)fh * fwt * sizeof(float2) + sizeof(WarpStarts);
   if (fixed + per_tilt > budget + 64 * 1024) return false;
   int chunk = (int)std::max<size_t>(1, (budget > fixed ? budget - fixed : 0) / per_tilt);
   chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
