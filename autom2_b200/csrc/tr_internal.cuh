@@ -117,6 +117,14 @@ struct WarpStarts {
   long long Wu[kThreads / 32], Wv[kThreads / 32];
 };
 
+// Forward-projection coordinate starts of one tilt: the x and z steps and,
+// per warp, U0 + wy A1 + wz kFNV A2 (V likewise); lane l's voxel pair starts
+// at W + 2 l A0.
+struct FpStarts {
+  long long A0, A2, B0, B2;
+  long long Wu[kThreads / 32], Wv[kThreads / 32];
+};
+
 // Separable rows (b1 = b3 = 0, b2 = 1): per voxel row of the tile, the lower
 // detector row and its weight, as the reference computes them.
 struct SepRow {

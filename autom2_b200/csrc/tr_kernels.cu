@@ -706,9 +706,11 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
                                         float *accs) {
   __shared__ TileTilt tt[kMaxChunk];
   __shared__ SepW sw[kMaxChunk][kTY];
+  __shared__ FpStarts fs[kMaxChunk];
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
+  const int warp = tid >> 5;
   const int wy = (tid >> 5) % kTY;
   const int wz = (tid >> 5) / kTY;
   const int xc = bx * kFX, yc = by * kTY, zl = bz * kFTZ;
@@ -766,18 +768,30 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
-    if (tid < nc)
-      tile_setup(a.geo[a.t0 + c0 + tid], xc, yc, zc, a.ox, a.oy, a.oz, a.pny,
-                 SEP, kFX - 1, kTY - 1, kFTZ - 1, tt[tid], sw[tid]);
+    if (tid < nc) {
+      const TiltGeo &g = a.geo[a.t0 + c0 + tid];
+      tile_setup(g, xc, yc, zc, a.ox, a.oy, a.oz, a.pny, SEP, kFX - 1, kTY - 1, kFTZ - 1,
+                 tt[tid], sw[tid]);
+      FpStarts &st = fs[tid];
+      st.A0 = g.A[0];
+      st.A2 = g.A[2];
+      st.B0 = g.B[0];
+      st.B2 = g.B[2];
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) {
+        const int ry = w % kTY, rz = w / kTY;
+        st.Wu[w] = tt[tid].U0 + ry * g.A[1] + (long long)(rz * kFNV) * g.A[2];
+        st.Wv[w] = tt[tid].V0 + ry * g.B[1] + (long long)(rz * kFNV) * g.B[2];
+      }
+    }
     for (int e = tid; e < nc * per; e += kThreads) iacc[e] = 0;
     __syncthreads();
 
     for (int i = 0; i < nc && s_scale_nonzero; ++i) {
-      const TiltGeo &g = a.geo[a.t0 + c0 + i];
-      const long long A0 = g.A[0], A1 = g.A[1], A2 = g.A[2];
+      const FpStarts &st = fs[i];
+      const long long A0 = st.A0, A2 = st.A2;
       // Lane coordinates of the pair's voxels: A at x = xc + 2 lane, B at x+1.
-      unsigned long long UA = (unsigned long long)(tt[i].U0 + (2 * lane) * A0 +
-                                                   wy * A1 + (long long)(wz * kFNV) * A2);
+      unsigned long long UA = (unsigned long long)(st.Wu[warp] + (2 * lane) * A0);
       unsigned long long UB = UA + (unsigned long long)A0;
       if (SEP) {
         int *T = iacc + (size_t)(i * kTY + wy) * fw;
@@ -797,9 +811,8 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
           UB += (unsigned long long)A2;
         }
       } else {
-        const long long B0 = g.B[0], B1 = g.B[1], B2 = g.B[2];
-        unsigned long long VA = (unsigned long long)(tt[i].V0 + (2 * lane) * B0 +
-                                                     wy * B1 + (long long)(wz * kFNV) * B2);
+        const long long B0 = st.B0, B2 = st.B2;
+        unsigned long long VA = (unsigned long long)(st.Wv[warp] + (2 * lane) * B0);
         unsigned long long VB = VA + (unsigned long long)B0;
         int *T = iacc + (size_t)i * per;
 #pragma unroll
