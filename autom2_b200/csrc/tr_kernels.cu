@@ -578,17 +578,17 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
     fill_warp_starts(ws, tt + c0, a.geo + a.t0 + c0, nc, tid);
     const IT *R0 = raw0 + (size_t)buf * chunk * rs;
     const int ng = fw >> 2;  // four-entry groups per table row
-    EntryWalk w(tid, fh, ng);
-    for (int g = tid; g < nc * fh * ng; g += kThreads, w.next(fh, ng)) {
-      const int i = w.i, r = w.r, q = w.q << 2;  // q: the group's first column
-      const TileTilt &t = tt[c0 + i];
-      if (r >= t.nr || q >= t.nq) continue;
-      const IT *R = R0 + (size_t)i * rs;  // raw column = table column
-      const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
-      const int xs = t.kmin, ys = t.jmin;
-      const int x0 = xs + q;  // image column of the group's first entry
-      float p[5];
-      if (SEP) {
+    if constexpr (SEP) {
+      EntryWalk w(tid, fh, ng);
+      for (int g = tid; g < nc * fh * ng; g += kThreads, w.next(fh, ng)) {
+        const int i = w.i, r = w.r, q = w.q << 2;  // q: the group's first column
+        const TileTilt &t = tt[c0 + i];
+        if (r >= t.nr || q >= t.nq) continue;
+        const IT *R = R0 + (size_t)i * rs;  // raw column = table column
+        const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
+        const int xs = t.kmin, ys = t.jmin;
+        const int x0 = xs + q;  // image column of the group's first entry
+        float p[5];
         const SepW s = sw[c0 + i][r];
         const IT *r0 = R + (s.y0 - ys) * bw, *r1 = r0 + bw;
         const float w0 = s.w0 * sc, w1 = s.w1 * sc;
@@ -625,10 +625,22 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
             tbl2[(size_t)g * 4 + m] = make_float2(b - sl, sl);
           }
         }
-      } else {
+      }
+    } else {
+      // One four-entry group: tilt i of the chunk, table row r, first column q,
+      // group index g in the chunk's tables.
+      auto stage = [&](int i, int r, int q, int g) {
+        const IT *R = R0 + (size_t)i * rs;  // raw column = table column
+        float p[5];
+        if (MODE != BP_NORM) load5(R + r * bw + q, p);  // in the raw box for any r < fh
+        const TileTilt &t = tt[c0 + i];
+        if (r >= t.nr || q >= t.nq) return;
+        const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
+        const int xs = t.kmin, ys = t.jmin;
+        const int x0 = xs + q;  // image column of the group's first entry
         const int j = ys + r;
         if (MODE != BP_NORM || (x0 >= 0 && x0 + 4 <= pnx - 1 && j >= 0 && j <= pny - 1)) {
-          load5(R + r * bw + q, p);
+          if (MODE == BP_NORM) load5(R + r * bw + q, p);
 #pragma unroll
           for (int m = 0; m < 5; ++m) p[m] *= sc;
           store_group(tbl2 + (size_t)g * 4, p);
@@ -646,6 +658,17 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
             tbl2[(size_t)g * 4 + m] = make_float2(b - sl, sl);
           }
         }
+      };
+      // Each thread keeps one (row, group) position and stages it for the
+      // chunk's tilts, W tilts side by side when a table has fewer groups
+      // than the CTA has threads: the tilts' reads are independent.
+      const int P = fh * ng;  // groups per tilt
+      const int W = max(1, kThreads / P);
+      const int way = tid / P;
+      for (int pos = tid - way * P; way < W && pos < P; pos += kThreads) {
+        const int r = pos / ng, q = (pos - r * ng) << 2;
+#pragma unroll 2
+        for (int i = way; i < nc; i += W) stage(i, r, q, i * P + pos);
       }
     }
     __syncthreads();
