@@ -275,7 +275,8 @@ int run(const Options &o) {
   if (st == TR_OK)
     st = method == kMethodAdmm
              ? tr_admm_host(ctx, proj.data(), vol.data(), o.iteration, o.cgiter, o.gamma, o.soft)
-             : tr_reconstruct_host(ctx, method, proj.data(), vol.data(), o.iteration, o.gamma);
+             : tr_reconstruct_host(ctx, use_initial ? method : method | TR_RECON_ZERO_START,
+                                   proj.data(), vol.data(), o.iteration, o.gamma);
   if (st != TR_OK) {
     fprintf(stderr, "%s: %s\n", kProg, tr_last_error(ctx));
     tr_destroy(ctx);

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <complex>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -42,7 +43,15 @@ struct tr_ctx {
   float fp_nbound = 0;   // most voxel contributions per forward window entry
   TiltGeo *geo_d = nullptr;
 
-  // scratch
+  // scratch: buffers are kept across problems and grown on demand; slot
+  // records each buffer's capacity and the problem generation that last
+  // claimed it (set_problem starts a new generation)
+  struct Slot {
+    size_t cap = 0;
+    unsigned gen = 0;
+  };
+  std::map<void **, Slot> slots;
+  unsigned gen = 0;
   size_t scratch = 0;
   float *val_d = nullptr, *wt_d = nullptr, *wtvol_d = nullptr;
   void *res16_d = nullptr;      // 16-bit SIRT residual [ntilt][ny][nx]
@@ -85,41 +94,59 @@ tr_status cuda_fail(tr_ctx *c, cudaError_t e, const char *what) {
 size_t vol_elems(const tr_ctx *c) { return (size_t)c->nx * c->ny * c->th; }
 size_t proj_elems(const tr_ctx *c) { return (size_t)c->nx * c->ny * c->nt; }
 
+void scratch_free(tr_ctx *c, void **p) {
+  tr_ctx::Slot &sl = c->slots[p];
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+    c->scratch -= std::min(c->scratch, sl.cap);
+  }
+  sl.cap = 0;
+}
+
+// Frees the scratch buffers no call of the current problem has claimed.
+void release_idle(tr_ctx *c) {
+  for (auto &kv : c->slots)
+    if (*kv.first && kv.second.gen != c->gen) scratch_free(c, kv.first);
+}
+
+// Claims scratch buffer *p with at least `bytes` for the current problem:
+// reuses it when large enough, else reallocates it.  When the budget or the
+// device runs short, buffers idle in this problem are released first.
 tr_status scratch_alloc(tr_ctx *c, void **p, size_t bytes, const char *what) {
-  if (*p) return TR_OK;
+  tr_ctx::Slot &sl = c->slots[p];
+  if (*p && sl.cap >= bytes) {
+    sl.gen = c->gen;
+    return TR_OK;
+  }
+  if (*p) scratch_free(c, p);
+  if (c->budget && c->scratch + bytes > c->budget) release_idle(c);
   if (c->budget && c->scratch + bytes > c->budget)
     return fail(c, TR_ERR_BUDGET,
                 "%s needs %zu bytes; %zu of the %zu-byte budget in use", what,
                 bytes, c->scratch, c->budget);
   cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    release_idle(c);
+    e = cudaMalloc(p, bytes);
+  }
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
     return fail(c, TR_ERR_OOM, "cudaMalloc(%zu) for %s: %s", bytes, what,
                 cudaGetErrorString(e));
   }
+  sl.cap = bytes;
+  sl.gen = c->gen;
   c->scratch += bytes;
   return TR_OK;
 }
 
-void scratch_free(tr_ctx *c, void **p, size_t bytes) {
-  if (*p) {
-    cudaFree(*p);
-    *p = nullptr;
-    c->scratch -= std::min(c->scratch, bytes);
-  }
-}
-
+// Ends the current problem.  Its scratch buffers stay allocated for the next
+// problem to reuse (a new generation: they count as idle until claimed).
 void release_problem(tr_ctx *c) {
-  const size_t pb = proj_elems(c) * sizeof(float);
-  scratch_free(c, (void **)&c->val_d, pb);
-  scratch_free(c, (void **)&c->wt_d, pb);
-  scratch_free(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float));
-  scratch_free(c, (void **)&c->res16_d, proj_elems(c) * 2);
-  scratch_free(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt);
-  scratch_free(c, (void **)&c->rscale_d, sizeof(float) * c->nt);
-  scratch_free(c, (void **)&c->admm_d, 7 * vol_elems(c) * sizeof(float));
-  scratch_free(c, (void **)&c->admm_dot_d, (kAdmmParts + 3) * sizeof(double));
+  ++c->gen;
   if (c->geo_d) {
     cudaFree(c->geo_d);
     c->geo_d = nullptr;
@@ -216,14 +243,17 @@ FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
 
 // Kernel spectrum of the R-weighting filter for rows of nx samples.
 tr_status build_filter(tr_ctx *c, int nx) {
-  if (c->filt_nx == nx && c->ghat_d) return TR_OK;
+  if (c->filt_nx == nx && c->ghat_d && c->tw_d) {  // cached: claim for this problem
+    c->slots[(void **)&c->ghat_d].gen = c->slots[(void **)&c->tw_d].gen = c->gen;
+    return TR_OK;
+  }
   RweightSpectrum sp;
   if (!rweight_spectrum(nx, kSmemMax, &sp))
     return fail(c, TR_ERR_UNSUPPORTED, "row length %d needs an FFT of %d points", nx,
                 1 << sp.log2m);
   const int M = 1 << sp.log2m;
-  if (c->ghat_d) scratch_free(c, (void **)&c->ghat_d, sizeof(float2) << c->filt_log2m);
-  if (c->tw_d) scratch_free(c, (void **)&c->tw_d, sizeof(float2) << (c->filt_log2m - 1));
+  scratch_free(c, (void **)&c->ghat_d);
+  scratch_free(c, (void **)&c->tw_d);
   tr_status s = scratch_alloc(c, (void **)&c->ghat_d, sizeof(float2) * M, "filter spectrum");
   if (s) return s;
   s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * (M / 2), "filter twiddles");
@@ -278,17 +308,17 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
 }
 
 // Device copies of the host-buffer calls' stack and volume, kept across calls
-// of the same size.
+// and grown when a problem needs more.
 tr_status host_buffers(tr_ctx *c) {
   const size_t pn = proj_elems(c), vn = vol_elems(c);
-  if (c->hproj_n != pn) {
+  if (c->hproj_n < pn) {
     if (c->hproj_d) cudaFree(c->hproj_d);
     c->hproj_d = nullptr;
     c->hproj_n = 0;
     TR_CUDA(c, cudaMalloc(&c->hproj_d, pn * sizeof(float)));
     c->hproj_n = pn;
   }
-  if (c->hvol_n != vn) {
+  if (c->hvol_n < vn) {
     if (c->hvol_d) cudaFree(c->hvol_d);
     c->hvol_d = nullptr;
     c->hvol_n = 0;
@@ -418,8 +448,7 @@ tr_status tr_destroy(tr_ctx *c) {
   cudaSetDevice(c->device);
   cudaDeviceSynchronize();
   release_problem(c);
-  scratch_free(c, (void **)&c->ghat_d, 0);
-  scratch_free(c, (void **)&c->tw_d, 0);
+  for (auto &kv : c->slots) scratch_free(c, kv.first);
   if (c->hproj_d) cudaFree(c->hproj_d);
   if (c->hvol_d) cudaFree(c->hvol_d);
   if (c->io_stream) cudaStreamDestroy(c->io_stream);
@@ -807,8 +836,13 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   const size_t pn = proj_elems(c), vn = vol_elems(c);
   if ((st = host_buffers(c))) return st;
   cudaStream_t s = c->io_stream;
+  const bool zero_start = (method & TR_RECON_ZERO_START) != 0;
+  method &= ~TR_RECON_ZERO_START;
   TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice, s));
-  TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));
+  if (zero_start)
+    TR_CUDA(c, cudaMemsetAsync(c->hvol_d, 0, vn * sizeof(float), s));
+  else
+    TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));
   switch (method) {
     case TR_METHOD_BPT: st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s); break;
     case TR_METHOD_WBP: st = tr_wbp(c, c->hproj_d, c->hvol_d, s); break;

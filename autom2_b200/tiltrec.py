@@ -35,6 +35,7 @@ from . import build as _build
 
 LAYOUT_Y, LAYOUT_Z = 0, 1
 METHOD_BPT, METHOD_WBP, METHOD_SIRT, METHOD_SART, METHOD_FBP = 0, 1, 2, 3, 4
+RECON_ZERO_START = 0x100  # tr_reconstruct_host: start from zeros
 METHODS = {"BPT": METHOD_BPT, "WBP": METHOD_WBP, "SIRT": METHOD_SIRT,
            "SART": METHOD_SART, "FBP": METHOD_FBP}
 DTYPE_F32, DTYPE_F16, DTYPE_BF16 = 0, 1, 2
@@ -275,9 +276,12 @@ class Engine:
                     "tr_wbp")
 
     def reconstruct_host(self, method, proj: np.ndarray, vol: np.ndarray, iters=0,
-                         gamma=0.0):
-        """Host buffers in, host volume out (vol is updated in place)."""
+                         gamma=0.0, zero_start=False):
+        """Host buffers in, host volume out (vol is updated in place).
+        zero_start: start from a zero volume without reading vol."""
         m = METHODS[method] if isinstance(method, str) else int(method)
+        if zero_start:
+            m |= RECON_ZERO_START
         assert proj.dtype == np.float32 and proj.flags.c_contiguous
         assert vol.dtype == np.float32 and vol.flags.c_contiguous
         self._check(self.lib.tr_reconstruct_host(self.h, m, proj.ctypes.data,

@@ -64,6 +64,11 @@ typedef enum {
   TR_METHOD_FBP = 4    /* Shepp-Logan FBP filter + BPT       (--method FBP) */
 } tr_method;
 
+/* Flag OR-ed into tr_reconstruct_host's method: start from a zero volume
+ * (the reference's default without --initial); vol_host is then output only
+ * and is not copied to the device. */
+#define TR_RECON_ZERO_START 0x100
+
 /* Element types of 16-bit storage (projections, SIRT residuals). */
 typedef enum {
   TR_DTYPE_F32 = 0,
@@ -86,7 +91,13 @@ tr_status tr_geometry_from_angles(const float *angles_deg, int ntilt,
 
 /* Context on CUDA device `device` with a scratch budget in bytes (0 = none).
  * Replaces InitializeCuda (src/TiltRec/src/main/main-cuda.cpp:83-109) minus
- * its cudaDeviceReset. */
+ * its cudaDeviceReset.  Scratch buffers (reprojections, weights, filter
+ * spectra, host-call staging) are kept across tr_set_problem calls and
+ * reused when large enough, so a context that reconstructs many series
+ * allocates only when a larger one arrives; under a budget, or when the
+ * device is short of memory, buffers the current problem has not used are
+ * released first.  tr_scratch_bytes reports the budgeted buffers held;
+ * tr_destroy frees everything. */
 tr_status tr_create(int device, size_t hbm_budget, tr_ctx **out);
 tr_status tr_destroy(tr_ctx *ctx);
 const char *tr_last_error(const tr_ctx *ctx);
@@ -193,10 +204,12 @@ tr_status tr_wbp(tr_ctx *ctx, float *proj_dev, float *vol_dev, void *stream);
 
 /* Host-buffer reconstruction, the path a drop-in CLI takes: copies the
  * projections from host memory, reconstructs with `method` starting from
- * vol_host (BPT/WBP add to it; pass zeros for a fresh volume) and copies the
- * volume back; returns when vol_host holds the result.  Pinned host buffers
- * give the fastest copies.  Device buffers are kept in the context and reused
- * across calls of the same size. */
+ * vol_host (BPT/WBP add to it) -- or from zeros when method carries
+ * TR_RECON_ZERO_START, without reading vol_host -- and copies the volume
+ * back; returns when vol_host holds the result.  Pinned host buffers give the
+ * fastest copies.  Device buffers are kept in the context and reused across
+ * calls of the same size.  (main-cuda.cpp's read / CuSIRT / write sequence;
+ * the reference starts from zeros unless --initial is given.) */
 tr_status tr_reconstruct_host(tr_ctx *ctx, int method, const float *proj_host,
                               float *vol_host, int iters, float gamma);
 

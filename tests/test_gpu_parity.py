@@ -210,6 +210,53 @@ def test_host_buffer_path(engine, golden):
     vol[:] = 0
     engine.reconstruct_host("SIRT", g("proj").copy(), vol, 5, 0.5)
     assert O.rel_l2(vol, g("sirt5")) < TOL
+    # Zero start: the host volume is output only (NaNs in it are not read).
+    want = vol.copy()
+    for method, iters, ref in (("WBP", 0, "wbp"), ("SIRT", 5, "sirt5")):
+        vol[:] = np.nan
+        engine.reconstruct_host(method, g("proj").copy(), vol, iters, 0.5, zero_start=True)
+        assert np.isfinite(vol).all()
+        assert O.rel_l2(vol, g(ref)) < TOL
+    np.testing.assert_array_equal(vol, want)
+
+
+def _recon_host(eng, golden, name, method, iters):
+    nx, ny, nt, th, org = _dims(golden, name)
+    g = lambda k: golden[f"{name}/{k}"]  # noqa: E731
+    eng.set_problem(nx, ny, nt, th, g("coeff8"), T.LAYOUT_Y, org)
+    vol = np.empty((ny, th, nx), np.float32)
+    eng.reconstruct_host(method, g("proj").copy(), vol, iters, 0.5, zero_start=True)
+    return vol
+
+
+@pytest.mark.parametrize("budgeted", [False, True])
+def test_scratch_reuse_across_problems(golden, budgeted):
+    """A context keeps its scratch buffers across problems.  Alternating SIRT
+    on one series with WBP on another reuses them (no growth after the first
+    round); under a budget that fits only the SIRT buffers, the buffers idle
+    in the current problem make room (WBP's filter spectrum displaces them,
+    and SIRT takes the room back).  The volumes match fresh contexts'."""
+    jobs = (("cfg0s4", "SIRT", 5), ("ygen", "WBP", 0))
+    want = {}
+    for name, method, iters in jobs:
+        fresh = T.Engine(0)
+        want[name] = _recon_host(fresh, golden, name, method, iters)
+        fresh.close()
+    assert O.rel_l2(want["cfg0s4"], golden["cfg0s4/sirt5"]) < TOL
+    assert O.rel_l2(want["ygen"], golden["ygen/wbp"]) < TOL
+    eng = T.Engine(0)
+    _recon_host(eng, golden, *jobs[0])
+    need = eng.scratch_bytes
+    eng.close()
+    eng = T.Engine(0, hbm_budget=need if budgeted else 0)
+    held = []
+    for _ in range(2):
+        for name, method, iters in jobs + jobs[:1]:
+            assert O.rel_l2(_recon_host(eng, golden, name, method, iters), want[name]) < 1e-6
+        held.append(eng.scratch_bytes)
+    assert held[1] == held[0]
+    assert held[0] <= need if budgeted else held[0] > need
+    eng.close()
 
 
 def test_errors_are_reported(engine):
