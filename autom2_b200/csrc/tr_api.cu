@@ -22,7 +22,9 @@ using namespace trb;
 
 namespace {
 constexpr size_t kSmemBp = 64 * 1024;  // interpolation tables per CTA
-constexpr size_t kSmemFp = 48 * 1024;  // splat windows per CTA
+// Splat windows per CTA: with the kernel's ~8.4 KB of static bookkeeping, four
+// CTAs fit on an SM.
+constexpr size_t kSmemFp = 44 * 1024;
 constexpr size_t kSmemMax = 200 * 1024;
 }  // namespace
 

@@ -724,12 +724,23 @@ __global__ void __launch_bounds__(kThreads, 4)
 // within +-60 degrees); the sums are exact and independent of atomic order.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
+// A forward-projection CTA's shared bookkeeping.  Declared once per kernel and
+// passed in, so that a kernel instantiating both fp_tile forms holds one copy.
+struct FpShared {
+  TileTilt tt[kMaxChunk];
+  SepW sw[kMaxChunk][kTY];
+  FpStarts fs[kMaxChunk];
+  unsigned wmax[kThreads / 32];
+  float scale, inv;
+  int nonzero;
+};
+
 template <bool SEP>
 __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
-                                        float *accs) {
-  __shared__ TileTilt tt[kMaxChunk];
-  __shared__ SepW sw[kMaxChunk][kTY];
-  __shared__ FpStarts fs[kMaxChunk];
+                                        float *accs, FpShared &sh) {
+  TileTilt *const tt = sh.tt;
+  SepW(*const sw)[kTY] = sh.sw;
+  FpStarts *const fs = sh.fs;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -755,9 +766,9 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
     }
   }
   // Tile scale: largest |v| over the tile (as ordered float bits).
-  __shared__ unsigned wmax[kThreads / 32];
-  __shared__ float s_scale, s_inv;
-  __shared__ int s_nonzero;
+  unsigned *const wmax = sh.wmax;
+  float &s_scale = sh.scale, &s_inv = sh.inv;
+  int &s_nonzero = sh.nonzero;
   {
     unsigned m = 0;
 #pragma unroll
@@ -904,7 +915,8 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
 template <bool SEP>
 __global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
   extern __shared__ float accs[];
-  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs);
+  __shared__ FpShared sh;
+  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs, sh);
 }
 
 // SIRT residual (main/main-mpi.cpp:640-647): r = p - (wt != 0 ? val/wt : val),
@@ -1138,6 +1150,7 @@ __global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
   extern __shared__ float accs[];
   __shared__ long long s_tile;
   __shared__ int s_item;
+  __shared__ FpShared sh;
   const long long total = T->h.fp_tiles;
   const int n = T->h.nfp;
   for (;;) {
@@ -1155,8 +1168,8 @@ __global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
     const int bx = (int)(l % it.gx);
     l /= it.gx;
     const int by = (int)(l % it.gy), bz = (int)(l / it.gy);
-    if (it.sep) fp_tile<true>(it.a, bx, by, bz, accs);
-    else fp_tile<false>(it.a, bx, by, bz, accs);
+    if (it.sep) fp_tile<true>(it.a, bx, by, bz, accs, sh);
+    else fp_tile<false>(it.a, bx, by, bz, accs, sh);
   }
 }
 

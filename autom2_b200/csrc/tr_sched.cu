@@ -44,7 +44,7 @@ using namespace trb;
 
 namespace {
 
-constexpr size_t kSchedSmemFp = 48 * 1024;
+constexpr size_t kSchedSmemFp = 44 * 1024;  // four FP CTAs per SM with the static bookkeeping
 constexpr size_t kSchedSmemMax = 200 * 1024;
 
 double now_s() {

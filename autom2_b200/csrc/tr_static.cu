@@ -38,7 +38,7 @@ constexpr size_t kStaticScratchBytes = 64ull << 20;
 constexpr int kStaticMaxTilts = 360;
 constexpr int kStaticMaxDevices = 64;
 constexpr size_t kStaticSmemBp = 64 * 1024;
-constexpr size_t kStaticSmemFp = 48 * 1024;
+constexpr size_t kStaticSmemFp = 44 * 1024;
 constexpr size_t kStaticSmemMax = 200 * 1024;
 
 }  // namespace
