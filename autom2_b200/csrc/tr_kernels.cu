@@ -674,7 +674,8 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
     __syncthreads();
     if (tid == 0 && c + 2 < nchunks) issue(c + 2, buf);
     bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tblf, ws, nc, per, fw, pny, lane, wy, wz);
-    __syncthreads();
+    // No barrier here: the next chunk's tables and warp starts are written
+    // only after the CTA-wide __syncthreads_or that follows its copy wait.
   }
   uses[0] += (unsigned)(nchunks + 1) / 2;
   uses[1] += (unsigned)nchunks / 2;
