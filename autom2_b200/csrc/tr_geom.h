@@ -80,7 +80,9 @@ inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
   *bad_tilt = -1;
   out->fw = (int)std::ceil(span_u) + 4;
   out->fh = sep ? kTY : (int)std::ceil(span_v) + 5;
-  out->ffw = (int)std::ceil(fspan_u) + 4;
+  // Forward windows start at a 4-column boundary (up to 3 extra columns) and
+  // span whole 4-column groups, so that the flush adds 16-byte groups.
+  out->ffw = ((int)std::ceil(fspan_u) + 4 + 3 + 3) & ~3;
   out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5;
   out->sep = sep;
   out->nbound = fp_entry_bound(min_a1);

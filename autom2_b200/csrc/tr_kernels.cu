@@ -725,6 +725,13 @@ __global__ void __launch_bounds__(kThreads, 4)
 // within +-60 degrees); the sums are exact and independent of atomic order.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
+// Adds four floats to four consecutive global floats (16-byte aligned).
+__device__ __forceinline__ void red_add_v4(float *p, float x, float y, float z, float w) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(__cvta_generic_to_global(p)),
+               "f"(x), "f"(y), "f"(z), "f"(w)
+               : "memory");
+}
+
 // A forward-projection CTA's shared bookkeeping.  Declared once per kernel and
 // passed in, so that a kernel instantiating both fp_tile forms holds one copy.
 struct FpShared {
@@ -746,6 +753,9 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
+  // 16-byte pixel groups of the stack: rows and tilt planes of whole groups.
+  const bool vec_ok = ((a.pnx | (int)a.tstride) & 3) == 0 &&
+                      (reinterpret_cast<uintptr_t>(a.val) & 15) == 0;
   const int wy = (tid >> 5) % kTY;
   const int wz = (tid >> 5) / kTY;
   const int xc = bx * kFX, yc = by * kTY, zl = bz * kFTZ;
@@ -807,6 +817,11 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       const TiltGeo &g = a.geo[a.t0 + c0 + tid];
       tile_setup(g, xc, yc, zc, a.ox, a.oy, a.oz, a.pny, SEP, kFX - 1, kTY - 1, kFTZ - 1,
                  tt[tid], sw[tid]);
+      // Window column 0 on a 4-column boundary (the flush adds 4-pixel groups).
+      const int xs = tt[tid].kmin & ~3, o = tt[tid].kmin - xs;
+      tt[tid].U0 += (long long)o << 32;
+      tt[tid].nq += o;
+      tt[tid].kmin = xs;
       FpStarts &st = fs[tid];
       st.A0 = g.A[0];
       st.A2 = g.A[2];
@@ -885,37 +900,51 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
     __syncthreads();
 
     // Flush the windows: in-image pixels only, as the reference's splat.
+    // Four columns per thread: a group inside the image goes out as one
+    // 16-byte vector reduction when the stack's rows are 16-byte aligned;
+    // border groups add their in-image pixels one by one.
     for (int i = 0; i < nc; ++i) {
       const int kmin = tt[i].kmin, nq = tt[i].nq, nr = tt[i].nr;
       const int *T = iacc + (size_t)i * per;
       float *base = a.val + (size_t)(a.t0 + c0 + i) * a.tstride;
       const float inv = s_inv;
-      for (int r = tid >> 5; r < nr; r += kThreads / 32) {
-        for (int q = lane; q < nq; q += 32) {
-          const float s = (float)T[r * fw + q] * inv;
-          const int k = kmin + q;
-          if (s == 0.f || (unsigned)k >= (unsigned)a.pnx) continue;
-          if (SEP) {
-            const SepW w = sw[i][r];
-            if ((unsigned)w.y0 < (unsigned)a.pny)
-              atomicAdd(base + (size_t)w.y0 * a.pnx + k, s * (1 - w.dy));
-            if (w.dy != 0.f && (unsigned)(w.y0 + 1) < (unsigned)a.pny)
-              atomicAdd(base + (size_t)(w.y0 + 1) * a.pnx + k, s * w.dy);
+      const int ngq = (nq + 3) >> 2;
+      for (int e = tid; e < nr * ngq; e += kThreads) {
+        const int r = e / ngq, q = (e - r * ngq) << 2;
+        const int4 v = *reinterpret_cast<const int4 *>(T + r * fw + q);
+        const float s[4] = {(float)v.x * inv, (float)v.y * inv, (float)v.z * inv,
+                            (float)v.w * inv};
+        if (s[0] == 0.f && s[1] == 0.f && s[2] == 0.f && s[3] == 0.f) continue;
+        const int k = kmin + q;
+        const bool inside = vec_ok && k >= 0 && k + 3 < a.pnx;
+        auto add_row = [&](int j, float wgt) {
+          if ((unsigned)j >= (unsigned)a.pny) return;
+          float *p = base + (size_t)j * a.pnx + k;
+          if (inside && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            red_add_v4(p, s[0] * wgt, s[1] * wgt, s[2] * wgt, s[3] * wgt);
           } else {
-            const int j = tt[i].jmin + r;
-            if ((unsigned)j < (unsigned)a.pny)
-              atomicAdd(base + (size_t)j * a.pnx + k, s);
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+              if (s[m] != 0.f && (unsigned)(k + m) < (unsigned)a.pnx) atomicAdd(p + m, s[m] * wgt);
           }
+        };
+        if (SEP) {
+          const SepW w = sw[i][r];
+          add_row(w.y0, 1 - w.dy);
+          if (w.dy != 0.f) add_row(w.y0 + 1, w.dy);
+        } else {
+          add_row(tt[i].jmin + r, 1.f);
         }
       }
     }
+
     __syncthreads();
   }
 }
 
 template <bool SEP>
-__global__ void __launch_bounds__(kThreads) fp_kernel(const FpArgs a) {
-  extern __shared__ float accs[];
+__global__ void __launch_bounds__(kThreads, SEP ? 3 : 4) fp_kernel(const FpArgs a) {
+  extern __shared__ __align__(16) float accs[];
   __shared__ FpShared sh;
   fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs, sh);
 }
@@ -1148,7 +1177,7 @@ __global__ void quantize_batch_kernel(const BatchTable *T) {
 }
 
 __global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
-  extern __shared__ float accs[];
+  extern __shared__ __align__(16) float accs[];
   __shared__ long long s_tile;
   __shared__ int s_item;
   __shared__ FpShared sh;
