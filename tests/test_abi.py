@@ -33,6 +33,18 @@ def test_exports_every_declared_symbol(lib):
         assert hasattr(lib, n), n
 
 
+def test_header_constants_match_the_wrapper():
+    """The method codes and the zero-start flag the Python wrapper passes are
+    the header's."""
+    from autom2_b200 import tiltrec as T
+    text = open(os.path.join(ROOT, "include", "tiltrec_b200.h")).read()
+    flag = re.search(r"#define\s+TR_RECON_ZERO_START\s+(0x[0-9a-fA-F]+|\d+)", text)
+    assert flag and int(flag.group(1), 0) == T.RECON_ZERO_START
+    for name, code in re.findall(r"TR_METHOD_(\w+)\s*=\s*(\d+)", text):
+        assert T.METHODS[name] == int(code), name
+    assert not (T.RECON_ZERO_START & max(T.METHODS.values()))
+
+
 def test_geometry_matches_reference_vectors(golden, lib):
     ang = golden["geom/angles"]
     for par, c20 in zip(golden["geom/params"], golden["geom/coeff20"]):
