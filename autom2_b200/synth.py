@@ -83,12 +83,19 @@ def config(name: str, scale: int = 1) -> Config:
     return c
 
 
-def coefficients(cfg: Config) -> np.ndarray:
+def coefficients(cfg: Config, base=None) -> np.ndarray:
     """[ntilt][8] coefficients: the reference geometry for the tilt angles and
     XTILT, then the per-tilt detector shifts (a0, b0) and in-plane rotations
-    (rotating (a, b) about the origin) that the configuration adds."""
-    from .tiltrec import geometry_from_angles
-    c = geometry_from_angles(cfg.angles, 0.0, cfg.xtilt, 0.0).copy()
+    (rotating (a, b) about the origin) that the configuration adds.
+
+    ``base(angles, offset, pitch, zshift) -> [ntilt][8]`` computes the
+    reference geometry; by default the engine's ``tr_geometry_from_angles``.
+    The CPU reference arm of the benchmark passes the reference's own
+    TranslateAngleToCoefficients / DecorateCoefficients instead, so that it
+    never loads the engine."""
+    if base is None:
+        from .tiltrec import geometry_from_angles as base
+    c = np.array(base(cfg.angles, 0.0, cfg.xtilt, 0.0), dtype=np.float64).reshape(-1, 8)
     rng = np.random.default_rng(cfg.seed + 1000)
     nt = cfg.ntilt
     if cfg.rotation_sigma:

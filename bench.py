@@ -192,9 +192,21 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
+    import oracle
     from autom2_b200 import synth
     cfg = synth.config("cfg1")
-    coeff = synth.coefficients(cfg)
+    # The geometry comes from the reference's own TranslateAngleToCoefficients
+    # and DecorateCoefficients (oracle/_ref), else the oracle restatement of
+    # them: this arm never loads the engine library.
+    if oracle.reference_available():
+        ref = oracle.Reference()
+
+        def base(a, o, p, z):
+            c20 = ref.coeffs20(a, o, p, z)
+            return np.concatenate([c20[:, 0:4], c20[:, 10:14]], axis=1)
+    else:
+        base = oracle.Restatement().coeffs
+    coeff = synth.coefficients(cfg, base=base)
     rng = np.random.default_rng(1)
     # The CPU arm reconstructs row samples of the same series shape; the
     # input values do not change its timing.
