@@ -12,7 +12,8 @@ Two oracles live here:
 * ``Reference`` -- the unmodified reference CPU sources
   (``src/TiltRec/src/main/main-mpi.cpp`` / ``main-mpiz.cpp``, ``mrcmx``,
   ``filter``) compiled by ``oracle/Makefile`` into ``oracle/_ref/`` with
-  test-only MPI / FFTW / OpenCV shims.  Present only where it was built.
+  test-only MPI / FFTW / OpenCV C-API shims (exact double-precision DFTs in
+  place of cuFFT and OpenCV's).  Present only where it was built.
 """
 from __future__ import annotations
 
@@ -196,6 +197,8 @@ class Reference:
         y.ref_coeffs.argtypes = [_f32p, C.c_int, C.c_float, C.c_float, C.c_float, _f64p]
         y.ref_filter_rweight.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         y.ref_filter_rweight.restype = C.c_int
+        y.ref_filter_fbp.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _f32p]
+        y.ref_filter_fbp.restype = C.c_int
         geo = [C.c_int, C.c_int, C.c_int, C.c_int, _f64p, C.c_float, C.c_float, C.c_float]
         y.ref_y_backproject.argtypes = geo + [_f32p, _f32p]
         y.ref_y_sirt.argtypes = geo + [_f32p, _f32p, C.c_int, C.c_float, C.c_int]
@@ -207,6 +210,8 @@ class Reference:
                                           _f64p, C.c_float, _f32p, C.c_int, C.c_int,
                                           C.c_int, C.c_float]
         y.ref_y_sirt_threaded.restype = C.c_double
+        y.ref_y_sirt_zslabs.argtypes = [C.c_int] + geo + [_f32p, _f32p, C.c_int, C.c_float]
+        y.ref_y_sirt_zslabs.restype = C.c_double
         z.ref_z_run.argtypes = [C.c_int] + geo + [_f32p, _f32p, C.c_int, C.c_float, C.c_char_p]
         z.ref_z_run.restype = C.c_int
         z.ref_z_admm.argtypes = geo + [_f32p, _f32p, C.c_int, C.c_int, C.c_float, C.c_float,
@@ -224,6 +229,16 @@ class Reference:
         nt, ny, nx = p.shape
         rc = self.y.ref_filter_rweight(nx, ny, nt, p)
         assert rc == 0
+        return p
+
+    def filter_fbp(self, proj, mode=0):
+        """The reference's FBP row filter (ApplyFilterInplace mode 0
+        Shepp-Logan, 1 Ram-Lak) of a copy of proj [nt][ny][nx], run through
+        the OpenCV C-API shim."""
+        p = _c(proj, np.float32).copy()
+        nt, ny, nx = p.shape
+        rc = self.y.ref_filter_fbp(mode, nx, ny, nt, p)
+        assert rc == 0, rc
         return p
 
     def y_backproject(self, nx, ny, nt, th, c20, origin, proj, vol):
@@ -262,6 +277,15 @@ class Reference:
         return self.y.ref_y_sirt_threaded(nthreads, nx, ny, nt, th, _c(c20, np.float64),
                                           pitch, _c(proj, np.float32), row0, nrows,
                                           iters, gamma)
+
+    def y_sirt_zslabs(self, nthreads, nx, ny, nt, th, c20, origin, proj, vol, iters,
+                      gamma):
+        """The reference's whole-volume SIRT on host threads over z-slabs
+        (exact; see ref_wrap.cpp).  Returns (volume, wall seconds)."""
+        v = _c(vol, np.float32).copy()
+        t = self.y.ref_y_sirt_zslabs(nthreads, nx, ny, nt, th, _c(c20, np.float64), *origin,
+                                     _c(proj, np.float32), v, iters, gamma)
+        return v, t
 
     def z_run(self, mode, nx, ny, nt, th, c20, origin, proj, vol, iters=0, gamma=0.0):
         """mode: 0 BPT, 2 WBP, 3 SIRT, 4 SART (Z layout, vol [th][ny][nx])."""

@@ -18,8 +18,11 @@
 #include <string.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -142,6 +145,16 @@ int ref_filter_rweight(int nx, int ny, int nt, float *proj) {
   return ApplyFilterInplace(s, proj, (size_t)ny, 2);
 }
 
+// ApplyFilterInplace modes 0 (Shepp-Logan) and 1 (Ram-Lak): the FBP row
+// filters, through the OpenCV C-API shim (exact DFTs).  proj: [nt][ny][nx].
+int ref_filter_fbp(int mode, int nx, int ny, int nt, float *proj) {
+  if (mode != 0 && mode != 1) return -2;
+  MrcStackM s;
+  header_only(s, nx, ny, nt);
+  QuietStdout q;
+  return ApplyFilterInplace(s, proj, (size_t)ny, mode);
+}
+
 #ifdef REF_LAYOUT_Y
 // Y layout: proj [nt][ny][nx], vol [ny][th][nx]; one rank owning every row.
 
@@ -254,6 +267,115 @@ double ref_y_sirt_threaded(int nthreads, int nx, int ny, int nt, int th,
   }
   for (auto &t : pool) t.join();
   auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+namespace {
+// Reusable barrier for a fixed set of threads (C++17 has no std::barrier).
+class Barrier {
+ public:
+  explicit Barrier(int n) : n_(n) {}
+  void wait() {
+    std::unique_lock<std::mutex> lk(m_);
+    const unsigned long g = gen_;
+    if (++count_ == n_) {
+      count_ = 0;
+      ++gen_;
+      cv_.notify_all();
+    } else {
+      cv_.wait(lk, [&] { return gen_ != g; });
+    }
+  }
+
+ private:
+  std::mutex m_;
+  std::condition_variable cv_;
+  int n_, count_ = 0;
+  unsigned long gen_ = 0;
+};
+}  // namespace
+
+// Whole-volume SIRT of the reference (SIRT, main-mpi.cpp:614-664) on host
+// threads, exact: the volume is split into z-slabs (thread r owns sections
+// [z0, z1), copied to a [ny][z1-z0][nx] buffer with the origin moved by z0),
+// and per tilt every thread runs the reference's Reproject on its slab into
+// its own reprojection planes; the planes are summed in thread order, the
+// residual is formed as the reference forms it, and every thread runs the
+// reference's UpdateWeightsByProjDiff on its slab; after all tilts each slab
+// takes the reference's update vol += valvol / wtvol * gamma.  Per voxel the
+// arithmetic is the reference's; only the order in which the forward splat's
+// contributions are added to a detector pixel differs (slab partial sums).
+// vol [ny][th][nx] is updated in place.  Returns wall seconds.
+double ref_y_sirt_zslabs(int nthreads, int nx, int ny, int nt, int th, const double *c20,
+                         float ox, float oy, float oz, const float *proj, float *vol,
+                         int iters, float gamma) {
+  std::vector<Coeff> c = to_coeffs(c20, nt);
+  nthreads = std::max(1, std::min(nthreads, th));
+  const size_t plane = (size_t)ny * nx;
+  struct Slab {
+    int z0, nz;
+    std::vector<float> v, valvol, wtvol, val, wt;
+  };
+  std::vector<Slab> sl(nthreads);
+  for (int r = 0; r < nthreads; ++r) {
+    Slab &s = sl[r];
+    const int base = th / nthreads, rem = th % nthreads;
+    s.z0 = r * base + std::min(r, rem);
+    s.nz = base + (r < rem ? 1 : 0);
+    s.v.resize(plane * s.nz);
+    for (int y = 0; y < ny; ++y)
+      memcpy(&s.v[(size_t)y * s.nz * nx], vol + ((size_t)y * th + s.z0) * nx,
+             sizeof(float) * (size_t)s.nz * nx);
+    s.valvol.resize(plane * s.nz);
+    s.wtvol.resize(plane * s.nz);
+    s.val.resize(plane);
+    s.wt.resize(plane);
+  }
+  std::vector<float> resid(plane);
+  Barrier bar(nthreads);
+  QuietStdout q;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (int r = 0; r < nthreads; ++r) {
+    pool.emplace_back([&, r]() {
+      Slab &s = sl[r];
+      Point3DF o{ox, oy, oz - (float)s.z0};
+      Volume v(0, 0, 0, nx, s.nz, ny, s.v.data());
+      const size_t n0 = plane * r / nthreads, n1 = plane * (r + 1) / nthreads;
+      const size_t size = plane * s.nz;
+      for (int it = 0; it < iters; ++it) {
+        std::fill(s.valvol.begin(), s.valvol.end(), 0.f);
+        std::fill(s.wtvol.begin(), s.wtvol.end(), 0.f);
+        for (int idx = 0; idx < nt; ++idx) {
+          std::fill(s.val.begin(), s.val.end(), 0.f);
+          std::fill(s.wt.begin(), s.wt.end(), 0.f);
+          Reproject(o, v, c[idx], s.val.data(), s.wt.data(), s.nz, ny, nx);
+          bar.wait();
+          const float *pd = proj + plane * idx;
+          for (size_t n = n0; n < n1; ++n) {
+            float val = 0.f, wt = 0.f;
+            for (int k = 0; k < nthreads; ++k) {
+              val += sl[k].val[n];
+              wt += sl[k].wt[n];
+            }
+            if (wt) val /= wt;
+            resid[n] = pd[n] - val;
+          }
+          bar.wait();
+          UpdateWeightsByProjDiff(o, resid.data(), s.valvol.data(), s.wtvol.data(), c[idx],
+                                  s.nz, ny, nx);
+        }
+        for (size_t i = size; i--;)
+          if (s.wtvol[i]) s.v[i] += s.valvol[i] / s.wtvol[i] * gamma;
+      }
+    });
+  }
+  for (auto &t : pool) t.join();
+  auto t1 = std::chrono::steady_clock::now();
+  for (int r = 0; r < nthreads; ++r)
+    for (int y = 0; y < ny; ++y)
+      memcpy(vol + ((size_t)y * th + sl[r].z0) * nx, &sl[r].v[(size_t)y * sl[r].nz * nx],
+             sizeof(float) * (size_t)sl[r].nz * nx);
   return std::chrono::duration<double>(t1 - t0).count();
 }
 #endif  // REF_LAYOUT_Y

@@ -1,7 +1,10 @@
 /* Test-only declarations of the OpenCV 1.x C-API names used by the reference
- * filter source (filter/filter_prj.cpp).  Only the FBP filter modes 0/1 call
- * them; the WBP mode 2 that the oracle exercises never does.  Every function
- * is defined in shim/opencv_abort.cpp to abort if it is ever reached. */
+ * filter source (filter/filter_prj.cpp), for its FBP filter modes 0/1.  The
+ * definitions (shim/opencv_c.cpp) implement the single-channel float subset
+ * those modes use -- images and matrices with regions of interest, sub-rect
+ * views, flips, copies, row DFTs in OpenCV's packed real-spectrum layout and
+ * their products -- with the DFTs evaluated exactly in double precision.
+ * Oracle infrastructure only. */
 #ifndef ORACLE_SHIM_OPENCV_CORE_C_H
 #define ORACLE_SHIM_OPENCV_CORE_C_H
 
@@ -9,17 +12,21 @@ typedef void CvArr;
 typedef struct CvRect { int x, y, width, height; } CvRect;
 typedef struct CvSize { int width, height; } CvSize;
 typedef struct CvScalar { double val[4]; } CvScalar;
+/* `type` carries ORC_MAT_MAGIC in its high 16 bits, which tells a matrix
+ * from an image (whose first field, nSize, is small). */
 typedef struct CvMat {
   int type, step;
   int *refcount, hdr_refcount;
   union { unsigned char *ptr; float *fl; double *db; } data;
   int rows, cols;
 } CvMat;
+typedef struct IplROI { int coi, xOffset, yOffset, width, height; } IplROI;
 typedef struct IplImage {
   int nSize, ID, nChannels, alphaChannel, depth;
   char colorModel[4], channelSeq[4];
   int dataOrder, origin, align, width, height;
-  void *roi, *maskROI, *imageId, *tileInfo;
+  IplROI *roi;
+  void *maskROI, *imageId, *tileInfo;
   int imageSize;
   char *imageData;
   int widthStep;
@@ -27,10 +34,13 @@ typedef struct IplImage {
   char *imageDataOrigin;
 } IplImage;
 
+#define ORC_MAT_MAGIC 0x42420000
 #define IPL_DEPTH_32F 32
 #define IPL_DEPTH_64F 64
 #define CV_32FC1 5
 #define CV_DXT_FORWARD 0
+#define CV_DXT_INVERSE 1
+#define CV_DXT_SCALE 2
 #define CV_DXT_INV_SCALE 3
 #define CV_DXT_ROWS 4
 

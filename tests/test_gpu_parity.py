@@ -295,6 +295,24 @@ def test_fbp_filter_widths(engine, restatement, nx, mode):
     assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fbp_filter_vs_reference(engine, reference, mode):
+    """The FBP row filter against the unmodified reference's
+    (ApplyFilterInplace modes 0/1 in oracle/_ref, OpenCV C-API shim with
+    exact DFTs), on a stack whose rows take the long mirrored extension."""
+    rng = np.random.default_rng(40 + mode)
+    nt, ny, nx = 3, 11, 256
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    c8 = T.geometry_from_angles(np.zeros(nt, np.float32))
+    engine.set_problem(nx, ny, nt, 4, c8, 0)
+    p = dev(proj)
+    engine.filter_fbp(p, mode)
+    want = reference.filter_fbp(proj, mode)
+    got = host(p)
+    assert O.rel_l2(got, want) < 1e-6
+    assert np.abs(got - want).max() <= 1e-6 * np.abs(want).max()
+
+
 @pytest.mark.parametrize("layout", [0, 1])
 def test_fbp_reconstruction(engine, restatement, layout):
     """--method FBP: Shepp-Logan filter then the back-projection, through the

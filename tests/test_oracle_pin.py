@@ -195,6 +195,22 @@ def test_fbp_filter_restatement_matches_dft_steps(restatement, mode, nx):
         assert np.abs(got[r] - want).max() <= 1e-5 * np.abs(want).max()
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("shape", [(2, 40, 64), (2, 7, 256), (1, 5, 300)])
+def test_fbp_filter_restatement_matches_reference(reference, restatement, mode, shape):
+    """The restatement's FBP filter equals the unmodified reference's
+    (ApplyFilterInplace modes 0/1, FileterProjectionSymmetrize) run in the
+    oracle with the OpenCV C-API shim: its image padding, 2-D symmetrisation,
+    mirrored extension (both branches: 256- and 300-wide rows take the long
+    one), DFT-domain product and crop."""
+    rng = np.random.default_rng(sum(shape) + mode)
+    proj = rng.normal(size=shape).astype(np.float32)
+    want = reference.filter_fbp(proj, mode)
+    got = restatement.filter_fbp(proj, mode)
+    assert O.rel_l2(got, want) < 1e-6
+    assert np.abs(got - want).max() <= 1e-6 * max(1.0, np.abs(want).max())
+
+
 def test_resample_bin_restatement(restatement):
     """Area binning: a block mean when the factor divides the size; with a
     remainder the cells still tile the image, so the means agree."""
