@@ -4,6 +4,9 @@ Outputs:
   autom2_b200/lib/libtiltrec_b200.so   C-ABI library (include/tiltrec_b200.h)
   autom2_b200/bin/TiltRec-cuda         drop-in CLI, Y layout
   autom2_b200/bin/TiltRecZ-cuda        drop-in CLI, Z layout
+  autom2_b200/bin/TiltRec-mpi          the same, mpi option dialect, Y layout
+  autom2_b200/bin/TiltRecZ-mpi         the same, mpi option dialect, Z layout
+  autom2_b200/bin/resample             drop-in binning step
 
 Kernels are compiled for sm_100a only.  Run: python -m autom2_b200.build
 """
@@ -74,11 +77,13 @@ def build_cli(force: bool = False) -> list[str]:
         return []
     os.makedirs(BINDIR, exist_ok=True)
     outs = []
-    for name, layout in (("TiltRec-cuda", 0), ("TiltRecZ-cuda", 1)):
+    for name, layout, mpi in (("TiltRec-cuda", 0, 0), ("TiltRecZ-cuda", 1, 0),
+                              ("TiltRec-mpi", 0, 1), ("TiltRecZ-mpi", 1, 1)):
         out = os.path.join(BINDIR, name)
         deps = srcs + [os.path.join(CLI, "mrc_io.h"), LIB]
         if force or not _newer(out, deps):
             _run(["g++", "-std=c++17", "-O2", f"-DTR_CLI_LAYOUT={layout}",
+                  f"-DTR_CLI_MPI_DIALECT={mpi}",
                   "-I", INCLUDE, "-I", CLI, "-o", out + ".tmp", *srcs,
                   "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
             os.replace(out + ".tmp", out)

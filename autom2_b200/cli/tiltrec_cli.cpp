@@ -9,10 +9,15 @@
 //   --f2b/-f (byte output)   --help/-h
 // (option parsing: TR/opts/opts.cpp:126-359, TR/opts/opts-mpi.h:114-284).
 //
-// Compiled twice: TR_CLI_LAYOUT=0 gives TiltRec-cuda (Y layout, output MRC
-// (X, thickness, Y), TR/main/main-cuda.cpp), TR_CLI_LAYOUT=1 gives
+// Compiled four times: TR_CLI_LAYOUT=0 gives TiltRec-cuda (Y layout, output
+// MRC (X, thickness, Y), TR/main/main-cuda.cpp), TR_CLI_LAYOUT=1 gives
 // TiltRecZ-cuda (Z layout, output MRC (X, Y, thickness),
-// TR/main/main-cudaz.cpp, which forces XTILT to 0, :163).
+// TR/main/main-cudaz.cpp, which forces XTILT to 0, :163); with
+// TR_CLI_MPI_DIALECT=1 the same two layouts answer to the names the GUI also
+// spawns, TiltRec-mpi and TiltRecZ-mpi (CommandChainManager.qml:167-170), and
+// take the mpi executables' option table (TR/opts/opts-mpi.h:114-128): long
+// --tiltfile only, --initial, no --f2b; the reference's -a / -x short options
+// reach assert(false) there (:279-280) and are an error (status 1) here.
 //
 // Semantics follow the reference CPU path (TiltRec-mpi / TiltRecZ-mpi), the
 // parity target: FP64 coefficients (main-mpi.cpp:85-183), the Y-layout origin
@@ -42,6 +47,9 @@
 #ifndef TR_CLI_LAYOUT
 #define TR_CLI_LAYOUT 0
 #endif
+#ifndef TR_CLI_MPI_DIALECT
+#define TR_CLI_MPI_DIALECT 0
+#endif
 
 namespace {
 
@@ -58,7 +66,8 @@ struct Options {
 
 // ADMM has no tr_method code: it takes two more parameters (tr_admm_host).
 constexpr int kMethodAdmm = -1;
-const char *kProg = TR_CLI_LAYOUT == 0 ? "TiltRec-cuda" : "TiltRecZ-cuda";
+const char *kProg = TR_CLI_MPI_DIALECT ? (TR_CLI_LAYOUT == 0 ? "TiltRec-mpi" : "TiltRecZ-mpi")
+                                       : (TR_CLI_LAYOUT == 0 ? "TiltRec-cuda" : "TiltRecZ-cuda");
 
 void usage() {
   printf(
@@ -79,6 +88,17 @@ void usage() {
 
 // 1 ok, 0 help, -1 error (GetOpts conventions).
 int parse(int argc, char **argv, Options *o) {
+#if TR_CLI_MPI_DIALECT
+  static option longopts[] = {{"help", no_argument, nullptr, 'h'},
+                              {"input", required_argument, nullptr, 'i'},
+                              {"output", required_argument, nullptr, 'o'},
+                              {"initial", required_argument, nullptr, 'n'},
+                              {"tiltfile", required_argument, nullptr, 't'},
+                              {"geometry", required_argument, nullptr, 'g'},
+                              {"method", required_argument, nullptr, 'm'},
+                              {nullptr, 0, nullptr, 0}};
+  const char *shortopts = "hi:o:n:g:m:a:x:";
+#else
   static option longopts[] = {{"help", no_argument, nullptr, 'h'},
                               {"input", required_argument, nullptr, 'i'},
                               {"output", required_argument, nullptr, 'o'},
@@ -90,8 +110,16 @@ int parse(int argc, char **argv, Options *o) {
                               {"axis", required_argument, nullptr, 'a'},
                               {"f2b", no_argument, nullptr, 'f'},
                               {nullptr, 0, nullptr, 0}};
+  const char *shortopts = "hi:o:n:t:g:m:a:f";
+#endif
   int ch;
-  while ((ch = getopt_long(argc, argv, "hi:o:n:t:g:m:a:f", longopts, nullptr)) != -1) {
+  while ((ch = getopt_long(argc, argv, shortopts, longopts, nullptr)) != -1) {
+#if TR_CLI_MPI_DIALECT
+    if (ch == 'a' || ch == 'x') {  // assert(false) in the reference's GetOpts
+      fprintf(stderr, "%s: option -%c is not accepted\n", kProg, ch);
+      return -1;
+    }
+#endif
     switch (ch) {
       case 'h':
         usage();

@@ -5,7 +5,9 @@ built into oracle/_ref (one rank).  Both sides read the same MRC stack and
 tilt file; the output headers must match field for field (the statistics to
 float tolerance) and the volumes to relative L2 1e-5.  TiltRecZ-mpi's BPT and
 SIRT abort before writing their output (a double free in the reference), so
-those two are checked against the oracle restatement instead."""
+those two are checked against the oracle restatement instead.  The reference
+FBP filter needs OpenCV, which the oracle build provides as a test-only C-API
+shim with exact DFTs."""
 import os
 import subprocess
 
@@ -35,8 +37,8 @@ def case(tmp_path_factory):
     return d, proj, ang
 
 
-def ours(layout, *args):
-    exe = os.path.join(BIN, "TiltRec-cuda" if layout == 0 else "TiltRecZ-cuda")
+def ours(layout, *args, dialect="cuda"):
+    exe = os.path.join(BIN, ("TiltRec-" if layout == 0 else "TiltRecZ-") + dialect)
     r = subprocess.run([exe, *args], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr + r.stdout
     return r
@@ -138,18 +140,20 @@ def test_tiltrecz_vs_tiltrecz_mpi(case, method):
 
 
 @pytest.mark.parametrize("layout", [0, 1])
-def test_fbp_vs_oracle(case, restatement, layout):
-    """--method FBP: the reference's FBP filter needs OpenCV, which the
-    reference build here stubs out, so the executables are checked against the
-    oracle restatement (its filter is pinned to the reference's DFT steps in
-    test_oracle_pin.py)."""
+def test_fbp_vs_reference_mpi(case, restatement, layout):
+    """--method FBP against the reference's own TiltRec-mpi / TiltRecZ-mpi
+    (whose FBP filter runs through the oracle's OpenCV C-API shim, exact
+    DFTs), and against the oracle restatement."""
     d, proj, ang = case
     th = 10
-    out = d / f"fbp_{layout}.mrc"
-    geometry = f"0.5,{0 if layout else 1.5},0,{th}"
-    ours(layout, "--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
-         "--geometry", geometry, "--method", "FBP", "--output", str(out))
-    _, _, got = read_mrc(out)
+    a, b = d / f"fbp_{layout}.mrc", d / f"rfbp_{layout}.mrc"
+    geometry = f"0.5,0,0,{th}"
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", geometry, "--method", "FBP"]
+    ours(layout, *common, "--output", str(a))
+    reference(layout, *common, "--output", str(b))
+    compare(a, b)
+    _, _, got = read_mrc(a)
     assert O.rel_l2(got, restated(layout, proj, ang, geometry, "FBP")) < TOL
 
 
@@ -256,3 +260,34 @@ def test_resample_executable(case, restatement, tmp_path, mode):
     assert [int(v) for v in ho["m"]] == [want.shape[2], want.shape[1], want.shape[0]]
     for f in ("amin", "amax", "amean", "next"):
         assert np.array_equal(ho[f], hi[f]), f
+
+
+@pytest.mark.parametrize("layout,method,geometry", [
+    (0, "SIRT,2,0.5", "0,0,0,10"), (0, "WBP", "1.0,0,2.0,12"),
+    (1, "WBP", "1.0,0,2.0,12"), (1, "SART,1,0.4", "0,0,0,10")])
+def test_mpi_named_executables_vs_reference_mpi(case, layout, method, geometry):
+    """TiltRec-mpi / TiltRecZ-mpi, the names the GUI spawns for CPU runs, with
+    the mpi option dialect (--initial; --tiltfile long only), against the
+    reference's own -mpi executables given the same command line."""
+    d, proj, ang = case
+    th = int(geometry.split(",")[-1])
+    shape = (40, th, 64) if layout == 0 else (th, 40, 64)
+    init = np.random.default_rng(5).normal(size=shape).astype(np.float32) * 0.1
+    write_mrc(d / f"mi{layout}.mrc", init)
+    a, b = d / f"om_{layout}_{method}.mrc", d / f"rm_{layout}_{method}.mrc"
+    common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
+              "--geometry", geometry, "--method", method]
+    if method.startswith("S"):
+        common += ["--initial", str(d / f"mi{layout}.mrc")]
+    ours(layout, *common, "--output", str(a), dialect="mpi")
+    reference(layout, *common, "--output", str(b))
+    compare(a, b)
+
+
+def test_mpi_dialect_rejects_cuda_only_options(case):
+    d, _, _ = case
+    exe = os.path.join(BIN, "TiltRec-mpi")
+    for extra in (["--f2b"], ["-t", str(d / "a.rawtlt")], ["-a", "y"]):
+        r = subprocess.run([exe, "--input", str(d / "stack.mrc"), *extra], capture_output=True,
+                           text=True, timeout=60)
+        assert r.returncode != 0, extra
