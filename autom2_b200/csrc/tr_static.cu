@@ -11,14 +11,22 @@
 // device array of kStaticScratchBytes (64 MiB).
 //
 // The array is reserved on a device when this file's device module is loaded
-// there -- with CUDA's lazy module loading, at this entry point's first call on
-// that device -- and stays reserved until the process exits.  That first call
-// also looks up the array's device address (cudaGetSymbolAddress, with the
-// device current); make it before any stream capture.  Every call shares the
-// one array and leaves the last call's contents in it: the buffers that must
-// start at zero are cleared by each call, and calls whose work overlaps on the
-// GPU (different streams, or different host threads) race on the scratch and
-// must be serialised by the caller.
+// there -- with CUDA's lazy module loading (the default), at the first call of
+// this library's kernels on that device; with CUDA_MODULE_LOADING=EAGER, when
+// the library is loaded, on every device the process uses, whether or not
+// this entry point is ever called -- and stays reserved until the process
+// exits.  The first call on a device also looks up the array's device address
+// (cudaGetSymbolAddress, with the device current); make it before any stream
+// capture.  Every call shares the one array and leaves the last call's
+// contents in it: the buffers that must start at zero are cleared by each
+// call, and calls whose work overlaps on the GPU (different streams, or
+// different host threads) race on the scratch and must be serialised by the
+// caller.
+//
+// The per-tilt geometry reaches the device as kernel arguments (a copy kernel
+// per 32 tilts), so the call reads no host memory after it returns.  A
+// back-projection whose bounded staging wait gives up sets a sticky word in
+// the array that stays set until tr_static_take_timeout reads it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,14 +80,14 @@ struct StaticGeom {
 };
 
 // Fixed-point steps and tile windows for the coefficients, as the context
-// path derives them; returns false when the geometry is outside what the
-// kernels stage.
-bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
-            StaticGeom *out) {
+// path derives them; returns the GeomStatus (GEOM_OK when the kernels can
+// stage the geometry).
+int derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
+           StaticGeom *out) {
   GeomInfo gi;
   int bad = -1;
-  if (derive_geometry(coeff8, nt, nx, ny, th, kStaticSmemMax, g, &gi, &bad) != GEOM_OK)
-    return false;
+  const int gs = derive_geometry(coeff8, nt, nx, ny, th, kStaticSmemMax, g, &gi, &bad);
+  if (gs != GEOM_OK) return gs;
   out->fw = gi.fw;
   out->fh = gi.fh;
   out->ffw = gi.ffw;
@@ -88,7 +96,21 @@ bool derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
   out->nbound = gi.nbound;
   out->chunk_bp = chunk_for(kStaticSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
   out->chunk_fp = chunk_for(kStaticSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
-  return true;
+  return GEOM_OK;
+}
+
+// Up to kGeoPerLaunch tilts' geometry passed by value as a kernel argument
+// (3.6 KB, under the 4 KB argument limit of every launch form).
+constexpr int kGeoPerLaunch = 32;
+struct GeoChunk {
+  TiltGeo g[kGeoPerLaunch];
+};
+
+__global__ void geo_upload_kernel(const GeoChunk c, int n, TiltGeo *dst) {
+  const int words = (int)(sizeof(TiltGeo) / sizeof(long long));
+  const long long *src = reinterpret_cast<const long long *>(c.g);
+  long long *out = reinterpret_cast<long long *>(dst);
+  for (int i = threadIdx.x; i < n * words; i += blockDim.x) out[i] = src[i];
 }
 
 tr_status run(int device, int nx, int ny, int nt, int th, int layout,
@@ -104,7 +126,9 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
 
   TiltGeo g[kStaticMaxTilts];
   StaticGeom sg;
-  if (!derive(coeff8, nt, nx, ny, th, g, &sg)) return TR_ERR_UNSUPPORTED;
+  const int gs = derive(coeff8, nt, nx, ny, th, g, &sg);
+  if (gs == GEOM_NONFINITE) return TR_ERR_ARG;  // as tr_set_problem
+  if (gs != GEOM_OK) return TR_ERR_UNSUPPORTED;
 
   void *base = nullptr;
   if (static_scratch(device, &base) != cudaSuccess) return TR_ERR_CUDA;
@@ -117,10 +141,13 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
 
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  // The pageable copy returns once `g` is staged, so the stack buffer may go.
-  if (cudaMemcpyAsync(geo, g, sizeof(TiltGeo) * nt, cudaMemcpyHostToDevice, s) !=
-      cudaSuccess)
-    return TR_ERR_CUDA;
+  for (int t0 = 0; t0 < nt; t0 += kGeoPerLaunch) {
+    GeoChunk c;
+    const int n = std::min(kGeoPerLaunch, nt - t0);
+    std::copy(g + t0, g + t0 + n, c.g);
+    geo_upload_kernel<<<1, 128, 0, s>>>(c, n, geo + t0);
+    if (cudaGetLastError() != cudaSuccess) return TR_ERR_CUDA;
+  }
 
   VolView v;
   v.vol = vol;
@@ -178,7 +205,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   bw.img.p = nullptr;
   bw.gamma = 1.f;
   bw.out = wtvol;
-  if (cudaMemsetAsync(flags, 0, 2 * sizeof(int), s) != cudaSuccess) return TR_ERR_CUDA;
+  if (cudaMemsetAsync(flags, 0, sizeof(int), s) != cudaSuccess) return TR_ERR_CUDA;
   if (launch_bp(BP_WEIGHTS, sg.sep, bw, s) != cudaSuccess) return TR_ERR_CUDA;
 
   for (int it = 0; it < iters; ++it) {
@@ -221,3 +248,46 @@ extern "C" tr_status tr_sirt_static(int device, int nx, int ny, int ntilt,
 }
 
 extern "C" size_t tr_static_scratch_limit(void) { return kStaticScratchBytes; }
+
+// Reads and clears the sticky device-wait word of the static scratch on
+// `device` (after the caller has synchronised the streams of its calls).
+extern "C" tr_status tr_static_take_timeout(int device) {
+  if (device < 0 || device >= kStaticMaxDevices) return TR_ERR_ARG;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return TR_ERR_CUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return TR_ERR_CUDA;
+  tr_status st = TR_OK;
+  void *base = nullptr;
+  int h = 0;
+  if (static_scratch(device, &base) != cudaSuccess ||
+      cudaMemcpy(&h, (int *)base + 1, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    st = TR_ERR_CUDA;
+  } else if (h) {
+    st = cudaMemset(base, 0, 2 * sizeof(int)) == cudaSuccess ? TR_ERR_TIMEOUT : TR_ERR_CUDA;
+  }
+  if (prev != device) cudaSetDevice(prev);
+  return st;
+}
+
+// The bounded device wait on the static scratch's words: one CTA waits on a
+// barrier nothing completes for budget_us of GPU clock, gives up and reports
+// as a back-projection would; the report is then read back as a timeout.
+extern "C" tr_status tr_static_selftest_wait(int device, int budget_us) {
+  if (device < 0 || device >= kStaticMaxDevices || budget_us < 1 || budget_us > 10000000)
+    return TR_ERR_ARG;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return TR_ERR_CUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return TR_ERR_CUDA;
+  void *base = nullptr;
+  int khz = 0;
+  tr_status st = TR_OK;
+  if (static_scratch(device, &base) != cudaSuccess ||
+      cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device) != cudaSuccess ||
+      cudaMemset(base, 0, 2 * sizeof(int)) != cudaSuccess ||
+      launch_bounded_wait_selftest((long long)khz * budget_us / 1000, (int *)base, nullptr) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(nullptr) != cudaSuccess)
+    st = TR_ERR_CUDA;
+  if (prev != device) cudaSetDevice(prev);
+  return st ? st : tr_static_take_timeout(device);
+}

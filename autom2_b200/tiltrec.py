@@ -346,6 +346,22 @@ def static_scratch_limit() -> int:
     return int(lib.tr_static_scratch_limit())
 
 
+def static_take_timeout(device=0) -> int:
+    """tr_static_take_timeout's status: TR_ERR_TIMEOUT (-5) when a
+    tr_sirt_static back-projection gave up a device wait since the last read."""
+    lib = load_library()
+    lib.tr_static_take_timeout.argtypes = [C.c_int]
+    return int(lib.tr_static_take_timeout(device))
+
+
+def static_selftest_wait(budget_us: int, device=0) -> int:
+    """tr_static_selftest_wait's status (-5 when the bounded wait gave up and
+    the report came back through the static scratch, as it should)."""
+    lib = load_library()
+    lib.tr_static_selftest_wait.argtypes = [C.c_int, C.c_int]
+    return int(lib.tr_static_selftest_wait(device, budget_us))
+
+
 # ------------------------------------------------------------ batched jobs
 
 class Job(C.Structure):

@@ -47,17 +47,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/<kernel>.md, line 'traffic_bytes_per_launch: N'), or None."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+# DRAM bytes per full cfg1 launch of the dominant kernels, from one ncu
+# capture each (dram__bytes_read.sum + dram__bytes_write.sum of a 512^2 x 61,
+# 512^2 x 128 case, scaled by component to the full launch: voxel-side bytes
+# x 8, detector-side bytes x 4).  The captures, their commands and the
+# scaling are summarised in profiles/fp_kernel.md and profiles/bp_kernel.md;
+# None where no capture of the current kernel exists yet.
+TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": None, "bp_kernel": None}
 
 
 class ClockSampler:
@@ -318,7 +314,7 @@ def run_ours(args):
     dominant = "fp_kernel" if fp_ms > bp_ms else "bp_kernel"
     kms, kbytes = (fp_ms, fp_bytes) if fp_ms > bp_ms else (bp_ms, bpn_bytes)
     achieved = kbytes / (kms / 1e3) / 1e9
-    traffic = profile_traffic(dominant)
+    traffic = TRAFFIC_BYTES_PER_LAUNCH.get(dominant)
     vpu_kernel = nt * nvox
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "kernel": dominant,

@@ -313,19 +313,38 @@ tr_status tr_sched_destroy(tr_sched *s);
  * device-wide synchronisation an allocation can imply.  Arguments are those of
  * tr_set_problem followed by those of tr_sirt; `device` is made current for
  * the call and restored.  All scratch lives in one static device array of
- * tr_static_scratch_limit() bytes (64 MiB), reserved on each device the first
- * time this is called there and held until the process exits; problems whose
- * geometry (ntilt*112 B), reprojection and projection weights
+ * tr_static_scratch_limit() bytes (64 MiB), held until the process exits.  It
+ * is reserved when the library's device code is loaded on a device: under
+ * CUDA's default lazy module loading at the first use of the library's kernels
+ * there; under CUDA_MODULE_LOADING=EAGER as soon as the library is loaded, on
+ * every device the process uses, whether or not this function is called.
+ * Problems whose geometry (ntilt*112 B), reprojection and projection weights
  * (2*ntilt*ny*nx*4 B) and voxel weights (voxels*4 B), each rounded up to
- * 256 B, exceed it are rejected with TR_ERR_BUDGET, and ntilt is at most 360.
- * The first call on a device looks up the array's device address; make it
- * before any stream capture.  Calls share the array: each clears what must
- * start at zero, and calls whose work overlaps on the GPU race. */
+ * 256 B, exceed it are rejected with TR_ERR_BUDGET, and ntilt is at most 360;
+ * non-finite coefficients give TR_ERR_ARG.  The geometry is passed to the
+ * device as kernel arguments, so nothing on the host is read after the call
+ * returns.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  Calls share the array: each clears what
+ * must start at zero, and calls whose work overlaps on the GPU race.  A
+ * back-projection whose bounded staging wait gives up leaves its volume
+ * unchanged and sets a sticky report word in the array that later calls do
+ * not clear: tr_static_take_timeout returns it. */
 tr_status tr_sirt_static(int device, int nx, int ny, int ntilt, int thickness,
                          int layout, const double *coeff8, float ox, float oy,
                          float oz, const float *proj_dev, float *vol_dev,
                          int iters, float gamma, void *stream);
 size_t tr_static_scratch_limit(void);
+/* Reads and clears the static scratch's device-wait report on `device`:
+ * TR_ERR_TIMEOUT when a tr_sirt_static back-projection gave up a wait since
+ * the last read, else TR_OK.  Synchronise the streams of the calls first.  No
+ * counterpart in the reference. */
+tr_status tr_static_take_timeout(int device);
+/* Self-test of the static path's device-wait report (no counterpart in the
+ * reference): a bounded wait on a barrier nothing completes, with a budget of
+ * budget_us microseconds of GPU clock, reporting through the static scratch;
+ * returns TR_ERR_TIMEOUT (the expected outcome) as tr_static_take_timeout
+ * would after a back-projection that gave up. */
+tr_status tr_static_selftest_wait(int device, int budget_us);
 
 /* Area binning of nt images [nt][ny][nx] to [nt][ny/bin][nx/bin] (bin 1..64),
  * the GUI chain's `resample -b bin` before TiltRec (resample/src/main/

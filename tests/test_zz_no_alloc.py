@@ -33,12 +33,23 @@ def test_static_sirt_matches_context_sirt_twice(golden):
     torch.cuda.synchronize()
     want = want.cpu().numpy()
     eng.close()
-    for _ in range(2):  # the second call starts from the first call's scratch
-        vol = torch.zeros((ny, th, nx), device="cuda")
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    for k in range(2):  # the second call starts from the first call's scratch
+        vol.zero_()
+        torch.cuda.synchronize()
+        # Device memory free before and after the call (driver view: every
+        # cudaMalloc of the process shows; torch allocates nothing here, the
+        # tensors exist already).
+        free0 = torch.cuda.mem_get_info()[0]
         T.sirt_static(proj, vol, c8, 5, 0.5, T.LAYOUT_Y, org)
         torch.cuda.synchronize()
-        assert O.rel_l2(vol.cpu().numpy(), want) < TOL
-        assert O.rel_l2(vol.cpu().numpy(), golden["cfg0s4/sirt5"]) < TOL
+        free1 = torch.cuda.mem_get_info()[0]
+        if k == 1:  # the first call may load the library's device code
+            assert free1 == free0, f"the call changed free device memory by {free0 - free1} B"
+        got = vol.cpu().numpy()
+        assert O.rel_l2(got, want) < TOL
+        assert O.rel_l2(got, golden["cfg0s4/sirt5"]) < TOL
+    assert T.static_take_timeout() == 0  # no device wait gave up
 
 
 def test_static_sirt_rejects_problems_beyond_its_scratch():
@@ -57,3 +68,22 @@ def test_static_sirt_rejects_problems_beyond_its_scratch():
     st = fn(0, nx, ny, nt, th, 0, np.ascontiguousarray(c8).ctypes.data_as(C.POINTER(C.c_double)),
             512.0, 32.0, 32.0, proj.data_ptr(), vol.data_ptr(), 1, 0.5, None)
     assert st == -3  # TR_ERR_BUDGET
+
+
+def test_static_sirt_reports_a_device_wait_that_gave_up():
+    # A bounded wait on a barrier nothing completes (50 ms), reporting through
+    # the static scratch as a back-projection does; the report stays until it
+    # is read, and reading clears it.
+    assert T.static_selftest_wait(50_000) == -5  # TR_ERR_TIMEOUT
+    assert T.static_take_timeout() == 0
+
+
+def test_static_sirt_rejects_non_finite_coefficients():
+    nt, ny, nx, th = 3, 8, 16, 4
+    c8 = np.tile([0, 1, 0, 0, 0, 0, 1, 0.0], (nt, 1))
+    c8[1, 3] = np.nan
+    proj = torch.zeros((nt, ny, nx), device="cuda")
+    vol = torch.zeros((ny, th, nx), device="cuda")
+    with pytest.raises(T.TiltRecError) as e:
+        T.sirt_static(proj, vol, c8, 1, 0.5, T.LAYOUT_Y)
+    assert e.value.status == -1  # TR_ERR_ARG, as tr_set_problem
