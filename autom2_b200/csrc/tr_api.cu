@@ -303,8 +303,8 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   c->ffh = gi.ffh;
   c->fp_nbound = gi.nbound;
   c->sep = gi.sep;
-  c->chunk_bp = chunk_for(kSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
-  c->chunk_fp = chunk_for(kSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
+  c->chunk_bp = chunk_for(kSmemBp, gi.bp_tilt_bytes);
+  c->chunk_fp = chunk_for(kSmemFp, gi.fp_tilt_bytes);
   c->wt_ready = c->wtvol_ready = false;
   return TR_OK;
 }

@@ -174,7 +174,7 @@ BpArgs job_bp(const tr_sched *S, const Job &j, const void *img, int dtype, const
   a.oz = j.d.oz;
   a.fw = j.gi.fw;
   a.fh = j.gi.fh;
-  a.chunk = chunk_for(64 * 1024, (size_t)j.gi.fw * j.gi.fh * sizeof(float2));
+  a.chunk = chunk_for(64 * 1024, j.gi.bp_tilt_bytes);
   a.gamma = gamma;
   a.wtvol = nullptr;
   a.out = nullptr;
@@ -197,7 +197,7 @@ FpArgs job_fp(const tr_sched *S, const Job &j, const float *vol, float *out) {
   a.oz = j.d.oz;
   a.fw = j.gi.ffw;
   a.fh = j.gi.ffh;
-  a.chunk = chunk_for(S->smem_fp, (size_t)j.gi.ffw * j.gi.ffh * sizeof(float));
+  a.chunk = chunk_for(S->smem_fp, j.gi.fp_tilt_bytes);
   a.nbound = j.gi.nbound;
   return a;
 }
@@ -342,7 +342,7 @@ tr_status admit(tr_sched *S, Job &j) {
     a.wtvol = j.wtvol;
     if (!batch_bp_layout(a, j.gi.sep, S->smem_bp, &j.bp_sirt, &j.smem_sirt) ||
         j.smem_sirt > S->smem_bp ||
-        (size_t)j.fp.a.chunk * j.gi.ffw * j.gi.ffh * sizeof(float) > S->smem_fp)
+        (size_t)j.fp.a.chunk * j.gi.fp_tilt_bytes > S->smem_fp)
       return sched_fail(S, TR_ERR_UNSUPPORTED, "tile window does not suit the step's layout");
     fill_grid(&j.bp_sirt, gb, BP_SIRT, j.gi.sep);
   }

@@ -94,8 +94,8 @@ int derive(const double *coeff8, int nt, int nx, int ny, int th, TiltGeo *g,
   out->ffh = gi.ffh;
   out->sep = gi.sep;
   out->nbound = gi.nbound;
-  out->chunk_bp = chunk_for(kStaticSmemBp, (size_t)gi.fw * gi.fh * sizeof(float2));
-  out->chunk_fp = chunk_for(kStaticSmemFp, (size_t)gi.ffw * gi.ffh * sizeof(float));
+  out->chunk_bp = chunk_for(kStaticSmemBp, gi.bp_tilt_bytes);
+  out->chunk_fp = chunk_for(kStaticSmemFp, gi.fp_tilt_bytes);
   return GEOM_OK;
 }
 
