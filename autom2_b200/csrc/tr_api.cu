@@ -258,10 +258,10 @@ tr_status build_filter(tr_ctx *c, int nx) {
   scratch_free(c, (void **)&c->tw_d);
   tr_status s = scratch_alloc(c, (void **)&c->ghat_d, sizeof(float2) * M, "filter spectrum");
   if (s) return s;
-  s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * (M / 2), "filter twiddles");
+  s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * M, "filter twiddles");
   if (s) return s;
   TR_CUDA(c, cudaMemcpy(c->ghat_d, sp.ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-  TR_CUDA(c, cudaMemcpy(c->tw_d, sp.tw.data(), sizeof(float2) * (M / 2), cudaMemcpyHostToDevice));
+  TR_CUDA(c, cudaMemcpy(c->tw_d, sp.tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
   c->filt_nx = nx;
   c->filt_npad = sp.npad;
   c->filt_log2m = sp.log2m;

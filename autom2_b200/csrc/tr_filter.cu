@@ -15,10 +15,11 @@
 // built once on the host in double precision.
 //
 // Per CTA: rows r and r+1 become the real and imaginary parts of one complex
-// sequence in shared memory; a radix-2 decimation-in-frequency pass sequence
-// (natural in, bit-reversed out), a pointwise product with the spectrum, and a
-// decimation-in-time inverse (bit-reversed in, natural out) give both filtered
-// rows at once because the kernel is real.
+// sequence of M points in shared memory; a Stockham autosort FFT (radix-4
+// passes, one radix-2 pass first when log2 M is odd; each thread holds its
+// butterflies' points in registers between a load and a store phase), a
+// pointwise product with the spectrum, and the inverse transform give both
+// filtered rows at once because the kernel is real.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,13 +31,78 @@ namespace trb {
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ float2 cmulc(float2 a, float2 b) {  // a * conj(b)
-  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+constexpr int kFftMaxB = 4;  // butterflies per thread and pass (launcher sizes the block)
+
+// One Stockham pass of radix R over buf[0..M) (M = 2^log2m), sub-transform
+// size Ns = 2^log2ns before the pass: butterfly j reads points j + r M/R,
+// multiplies point r by w^{r (j mod Ns)} with w = e^{DIR 2 pi i / (Ns R)},
+// transforms the R points and writes them to (j / Ns) Ns R + (j mod Ns) +
+// r Ns.  DIR = -1 forward, +1 inverse (unscaled).  tw[t] = e^{-2 pi i t / M}.
+template <int R, int DIR>
+__device__ __forceinline__ void stockham_pass(float2 *buf, int log2m, int log2ns,
+                                              const float2 *__restrict__ tw) {
+  const int M = 1 << log2m, nb = M / R, Ns = 1 << log2ns;
+  constexpr int lr = R == 4 ? 2 : 1;
+  float2 v[kFftMaxB][R];
+#pragma unroll
+  for (int b = 0; b < kFftMaxB; ++b) {
+    const int j = threadIdx.x + b * blockDim.x;
+    if (j < nb) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = buf[j + r * nb];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < kFftMaxB; ++b) {
+    const int j = threadIdx.x + b * blockDim.x;
+    if (j < nb) {
+      const int k = j & (Ns - 1);
+      const int step = k << (log2m - log2ns - lr);  // k M / (Ns R)
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(tw + ((r * step) & (M - 1)));
+        if (DIR > 0) w.y = -w.y;
+        v[b][r] = cmul(v[b][r], w);
+      }
+      float2 o[R];
+      if (R == 2) {
+        o[0] = cadd(v[b][0], v[b][1]);
+        o[1] = csub(v[b][0], v[b][1]);
+      } else {
+        const float2 y0 = cadd(v[b][0], v[b][2]), y1 = csub(v[b][0], v[b][2]);
+        const float2 y2 = cadd(v[b][1], v[b][3]), d = csub(v[b][1], v[b][3]);
+        // forward: -i d; inverse: +i d
+        const float2 y3 = DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
+        o[0] = cadd(y0, y2);
+        o[1] = cadd(y1, y3);
+        o[2] = csub(y0, y2);
+        o[3] = csub(y1, y3);
+      }
+      const int base = ((j - k) << lr) + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[base + r * Ns] = o[r];
+    }
+  }
+  __syncthreads();
 }
 
-__global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
+template <int DIR>
+__device__ __forceinline__ void stockham_fft(float2 *buf, int log2m, const float2 *tw) {
+  int ls = 0;
+  if (log2m & 1) {
+    stockham_pass<2, DIR>(buf, log2m, 0, tw);
+    ls = 1;
+  }
+  for (; ls < log2m; ls += 2) stockham_pass<4, DIR>(buf, log2m, ls, tw);
+}
+
+__global__ void __launch_bounds__(1024) rweight_kernel(const FilterArgs f) {
   extern __shared__ float2 buf[];
-  const int M = 1 << f.log2m, half = M >> 1;
+  const int M = 1 << f.log2m;
   const long long r0 = 2ll * blockIdx.x;
   const bool has1 = r0 + 1 < f.nrows;
   const float *x0 = f.rows + r0 * f.nx;
@@ -61,34 +127,10 @@ __global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
     buf[j] = make_float2(re, im);
   }
   __syncthreads();
-
-  // Forward DIF.
-  for (int h = half, ts = 1; h >= 1; h >>= 1, ts <<= 1) {
-    for (int b = threadIdx.x; b < half; b += blockDim.x) {
-      const int grp = b / h, pos = b - grp * h;
-      const int i0 = grp * 2 * h + pos, i1 = i0 + h;
-      const float2 u = buf[i0], v = buf[i1];
-      buf[i0] = make_float2(u.x + v.x, u.y + v.y);
-      buf[i1] = cmul(make_float2(u.x - v.x, u.y - v.y), __ldg(f.tw + pos * ts));
-    }
-    __syncthreads();
-  }
-  // Spectrum product (both in bit-reversed order).
-  for (int j = threadIdx.x; j < M; j += blockDim.x)
-    buf[j] = cmul(buf[j], __ldg(f.ghat + j));
+  stockham_fft<-1>(buf, f.log2m, f.tw);
+  for (int j = threadIdx.x; j < M; j += blockDim.x) buf[j] = cmul(buf[j], __ldg(f.ghat + j));
   __syncthreads();
-  // Inverse DIT.
-  for (int h = 1, ts = half; h < M; h <<= 1, ts >>= 1) {
-    for (int b = threadIdx.x; b < half; b += blockDim.x) {
-      const int grp = b / h, pos = b - grp * h;
-      const int i0 = grp * 2 * h + pos, i1 = i0 + h;
-      const float2 u = buf[i0];
-      const float2 v = cmulc(buf[i1], __ldg(f.tw + pos * ts));
-      buf[i0] = make_float2(u.x + v.x, u.y + v.y);
-      buf[i1] = make_float2(u.x - v.x, u.y - v.y);
-    }
-    __syncthreads();
-  }
+  stockham_fft<1>(buf, f.log2m, f.tw);
   float *y0 = f.rows + r0 * f.nx;
   for (int j = threadIdx.x; j < nx; j += blockDim.x) {
     const float2 z = buf[j];
@@ -104,7 +146,8 @@ cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s) {
       rweight_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const long long pairs = (f.nrows + 1) / 2;
-  const int threads = M >= 8192 ? 512 : 256;
+  // At most kFftMaxB butterflies per thread in a radix-2 pass (M/2 of them).
+  const int threads = std::min(1024, std::max(64, M / (2 * kFftMaxB)));
   rweight_kernel<<<(unsigned)pairs, threads, smem, s>>>(f);
   return cudaGetLastError();
 }

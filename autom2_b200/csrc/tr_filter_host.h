@@ -36,8 +36,8 @@ inline void fft_host(std::vector<std::complex<double>> &x) {
 struct RweightSpectrum {
   int npad = 0;   // padded row length nx + nx/10 of the reference
   int log2m = 0;  // FFT size 2^log2m >= npad + nx - 1
-  std::vector<float2> ghat;  // kernel spectrum, bit-reversed order, scaled 1/(M nx)
-  std::vector<float2> tw;    // twiddles e^{-2 pi i k / M}, k < M/2
+  std::vector<float2> ghat;  // kernel spectrum, natural order, scaled 1/(M nx)
+  std::vector<float2> tw;    // twiddles e^{-2 pi i k / M}, k < M
 };
 
 // False when the FFT would not fit `smem_max` bytes of complex floats.
@@ -48,7 +48,7 @@ inline bool rweight_spectrum(int nx, size_t smem_max, RweightSpectrum *out) {
   const int M = 1 << log2m;
   out->npad = N;
   out->log2m = log2m;
-  if ((size_t)M * sizeof(float2) > smem_max) return false;
+  if ((size_t)M * sizeof(float2) > smem_max || log2m > 14) return false;
   // Weights exactly as filter_prj.cpp:694-723 forms them (float arithmetic).
   const int r = (int)floor((float)N * 0.05f);
   const float sg = (float)N * 0.5f;
@@ -76,14 +76,11 @@ inline bool rweight_spectrum(int nx, size_t smem_max, RweightSpectrum *out) {
   for (int e = -(N - 1); e <= nx - 1; ++e) g[(e % M + M) % M] = h[(e % N + N) % N];
   fft_host(g);
   out->ghat.resize(M);
-  out->tw.resize(M / 2);
+  out->tw.resize(M);
   const double scale = 1.0 / ((double)M * nx);
-  for (int i = 0; i < M; ++i) {
-    int br = 0;
-    for (int b = 0; b < log2m; ++b) br |= ((i >> b) & 1) << (log2m - 1 - b);
-    out->ghat[i] = make_float2((float)(g[br].real() * scale), (float)(g[br].imag() * scale));
-  }
-  for (int k = 0; k < M / 2; ++k)
+  for (int i = 0; i < M; ++i)
+    out->ghat[i] = make_float2((float)(g[i].real() * scale), (float)(g[i].imag() * scale));
+  for (int k = 0; k < M; ++k)
     out->tw[k] = make_float2((float)cos(2.0 * M_PI * k / M), (float)-sin(2.0 * M_PI * k / M));
   return true;
 }

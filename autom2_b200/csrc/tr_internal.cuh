@@ -155,8 +155,8 @@ struct FilterArgs {
   long long nrows;
   int nx, n_pad;        // row length and the reference's padded length N
   int log2m;            // M = 1 << log2m
-  const float2 *ghat;   // [M] kernel spectrum, bit-reversed, scaled
-  const float2 *tw;     // [M/2] e^{-2 pi i k / M}
+  const float2 *ghat;   // [M] kernel spectrum, natural order, scaled
+  const float2 *tw;     // [M] e^{-2 pi i k / M}
 };
 
 // ------------------------------------------------------------ batched steps

@@ -231,9 +231,9 @@ tr_status ensure_filter(tr_sched *S, int nx, std::pair<float2 *, float2 *> *out)
   const int M = 1 << sp.log2m;
   float2 *g = nullptr, *t = nullptr;
   SCHED_CUDA(S, cudaMalloc(&g, sizeof(float2) * M));
-  SCHED_CUDA(S, cudaMalloc(&t, sizeof(float2) * (M / 2)));
+  SCHED_CUDA(S, cudaMalloc(&t, sizeof(float2) * M));
   SCHED_CUDA(S, cudaMemcpy(g, sp.ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-  SCHED_CUDA(S, cudaMemcpy(t, sp.tw.data(), sizeof(float2) * (M / 2), cudaMemcpyHostToDevice));
+  SCHED_CUDA(S, cudaMemcpy(t, sp.tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
   S->filt[nx] = {g, t};
   S->filt_h[nx] = sp;
   *out = {g, t};
