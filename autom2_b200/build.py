@@ -28,7 +28,7 @@ LIB = os.path.join(LIBDIR, "libtiltrec_b200.so")
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["tr_kernels.cu", "tr_filter.cu", "tr_api.cu", "tr_static.cu", "tr_sched.cu",
-              "tr_admm.cu"]
+              "tr_admm.cu", "tr_output.cu"]
 CLI_SOURCES = ["mrc_io.cpp", "tiltrec_cli.cpp"]
 
 

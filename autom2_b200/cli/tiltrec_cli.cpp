@@ -192,11 +192,15 @@ int rank_from_env() {
 // --f2b: the reference maps each Y slab of (up to) 64 rows to bytes with an
 // exponentially averaged mean and deviation (alpha 0.9, starting from 0),
 // clamps the z-score to +-10 and scales to 0..255, converting complete groups
-// of four values only (recon_y.cu:164-181, basic.cu:442-475).
-std::vector<unsigned char> to_bytes(const std::vector<float> &vol, size_t slab) {
+// of four values only (recon_y.cu:164-181, basic.cu:442-475); the Z-layout
+// drivers map the whole volume with its own mean and deviation (recon_z.cu:
+// 164-172).  Reconstructions other than ADMM do this on the device
+// (tr_volume_to_bytes through tr_reconstruct_to_sink); ADMM's host volume is
+// mapped here the same way.
+std::vector<unsigned char> to_bytes(const std::vector<float> &vol, size_t slab, float alpha) {
   std::vector<unsigned char> out(vol.size(), 0);
   float gmean = 0, gstd = 0;
-  const float alpha = 0.9f, sf = 10.f;
+  const float sf = 10.f;
   for (size_t s0 = 0; s0 < vol.size(); s0 += slab) {
     const size_t n = std::min(slab, vol.size() - s0);
     double sum = 0;
@@ -218,6 +222,33 @@ std::vector<unsigned char> to_bytes(const std::vector<float> &vol, size_t slab) 
       }
   }
   return out;
+}
+
+// Output file written block by block as the engine streams the volume back:
+// the header first (rewritten at the end with the statistics of the middle
+// section, which is captured as it passes), then the data in order.
+struct FileSink {
+  FILE *f = nullptr;
+  size_t es = 4;                  // bytes per voxel in the file
+  size_t mid_off = 0, mid_n = 0;  // middle section: first byte, voxels
+  std::vector<float> mid;
+};
+
+int file_sink(void *user, const void *data, size_t off, size_t len) {
+  FileSink *k = static_cast<FileSink *>(user);
+  if (fwrite(data, 1, len, k->f) != len) return 1;
+  const size_t a = std::max(off, k->mid_off), b = std::min(off + len, k->mid_off + k->mid_n * k->es);
+  for (size_t p = a; p < b; p += k->es) {
+    const unsigned char *src = static_cast<const unsigned char *>(data) + (p - off);
+    float v;
+    if (k->es == 1) {
+      v = (float)src[0];
+    } else {
+      memcpy(&v, src, sizeof v);
+    }
+    k->mid[(p - k->mid_off) / k->es] = v;
+  }
+  return 0;
 }
 
 int run(const Options &o) {
@@ -274,13 +305,14 @@ int run(const Options &o) {
   const float ox = nx * 0.5f, oy = zlayout ? ny * 0.5f : th * 0.5f, oz = th * 0.5f;
 
   const size_t nvox = (size_t)nx * ny * th;
-  std::vector<float> vol(nvox, 0.f);
+  std::vector<float> vol;  // the starting volume (--initial), or ADMM's output
   // The starting volume: TiltRec-mpi loads it for every method
   // (main-mpi.cpp:778-791); the Z-layout BPT/WBP start from zero
   // (main-mpiz.cpp BackProject/FBP zero the volume).
   const bool use_initial = !o.initial.empty() &&
                            !(zlayout && (method == TR_METHOD_BPT || method == TR_METHOD_WBP ||
                                          method == TR_METHOD_FBP));
+  if (use_initial || method == kMethodAdmm) vol.assign(nvox, 0.f);
   if (use_initial) {
     trcli::MrcHeader ih;
     if (!trcli::read_header(o.initial, &ih, &err)) return fprintf(stderr, "%s\n", err.c_str()), 1;
@@ -300,35 +332,61 @@ int run(const Options &o) {
     return fprintf(stderr, "%s: no CUDA device %d\n", kProg, device), 1;
   int st = tr_set_problem(ctx, nx, ny, nt, th, zlayout ? TR_LAYOUT_Z : TR_LAYOUT_Y, coeff.data(),
                           ox, oy, oz);
-  if (st == TR_OK)
-    st = method == kMethodAdmm
-             ? tr_admm_host(ctx, proj.data(), vol.data(), o.iteration, o.cgiter, o.gamma, o.soft)
-             : tr_reconstruct_host(ctx, use_initial ? method : method | TR_RECON_ZERO_START,
-                                   proj.data(), vol.data(), o.iteration, o.gamma);
-  if (st != TR_OK) {
-    fprintf(stderr, "%s: %s\n", kProg, tr_last_error(ctx));
-    tr_destroy(ctx);
-    return 1;
-  }
-  tr_destroy(ctx);
 
   // Output: Y layout MRC (X, thickness, Y), Z layout MRC (X, Y, thickness).
   trcli::MrcHeader out = zlayout ? trcli::new_volume_header(nx, ny, th, o.f2b)
                                  : trcli::new_volume_header(nx, th, ny, o.f2b);
   const size_t plane = (size_t)out.nx * out.ny;
   const size_t mid = (size_t)(int)(out.nz * .5);
-  bool ok;
-  if (o.f2b) {
-    const size_t slab = (size_t)nx * th * 64;  // 64-row slabs of the Y layout
-    std::vector<unsigned char> b = to_bytes(vol, slab);
-    std::vector<float> sec(plane);
-    for (size_t i = 0; i < plane; ++i) sec[i] = (float)b[mid * plane + i];
-    trcli::update_stats(&out, sec.data(), plane);
-    ok = trcli::write_volume(o.output, out, b.data(), b.size(), &err);
-  } else {
-    trcli::update_stats(&out, vol.data() + mid * plane, plane);
-    ok = trcli::write_volume(o.output, out, vol.data(), vol.size() * sizeof(float), &err);
+  // Byte slabs: 64 rows of the Y layout (EMA alpha 0.9; the reference's slab
+  // height is at least 64 rows, more where its device memory allows), or the
+  // whole Z volume (alpha 0).
+  const size_t slab = zlayout ? nvox : (size_t)nx * th * 64;
+  const float alpha = zlayout ? 0.f : 0.9f;
+  bool ok = true;
+  if (st == TR_OK && method == kMethodAdmm) {
+    st = tr_admm_host(ctx, proj.data(), vol.data(), o.iteration, o.cgiter, o.gamma, o.soft);
+    if (st == TR_OK) {
+      if (o.f2b) {
+        std::vector<unsigned char> b = to_bytes(vol, slab, alpha);
+        std::vector<float> sec(plane);
+        for (size_t i = 0; i < plane; ++i) sec[i] = (float)b[mid * plane + i];
+        trcli::update_stats(&out, sec.data(), plane);
+        ok = trcli::write_volume(o.output, out, b.data(), b.size(), &err);
+      } else {
+        trcli::update_stats(&out, vol.data() + mid * plane, plane);
+        ok = trcli::write_volume(o.output, out, vol.data(), vol.size() * sizeof(float), &err);
+      }
+    }
+  } else if (st == TR_OK) {
+    FileSink k;
+    k.f = fopen(o.output.c_str(), "wb");
+    if (!k.f) {
+      tr_destroy(ctx);
+      return fprintf(stderr, "%s: cannot create %s\n", kProg, o.output.c_str()), 1;
+    }
+    k.es = o.f2b ? 1 : sizeof(float);
+    k.mid_off = mid * plane * k.es;
+    k.mid_n = plane;
+    k.mid.assign(plane, 0.f);
+    ok = fwrite(&out, 1, sizeof out, k.f) == sizeof out;  // placeholder header
+    if (ok)
+      st = tr_reconstruct_to_sink(ctx, method, proj.data(), use_initial ? vol.data() : nullptr,
+                                  o.iteration, o.gamma, o.f2b ? slab : 0, alpha, 64u << 20,
+                                  file_sink, &k);
+    if (ok && st == TR_OK) {
+      trcli::update_stats(&out, k.mid.data(), plane);
+      ok = fseek(k.f, 0, SEEK_SET) == 0 && fwrite(&out, 1, sizeof out, k.f) == sizeof out;
+    }
+    ok = (fclose(k.f) == 0) && ok;
+    if (!ok) err = "write failed for " + o.output;
   }
+  if (st != TR_OK) {
+    fprintf(stderr, "%s: %s\n", kProg, tr_last_error(ctx));
+    tr_destroy(ctx);
+    return 1;
+  }
+  tr_destroy(ctx);
   if (!ok) return fprintf(stderr, "%s\n", err.c_str()), 1;
   printf("%s: %s %dx%dx%d tilts=%d -> %s\n", kProg, o.method.c_str(), nx, ny, th, nt,
          o.output.c_str());

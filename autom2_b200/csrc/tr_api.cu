@@ -66,6 +66,14 @@ struct tr_ctx {
   float2 *ghat_d = nullptr, *tw_d = nullptr;
   float *hproj_d = nullptr, *hvol_d = nullptr;
   size_t hproj_n = 0, hvol_n = 0;
+  // byte output: slab partial sums and statistics, the bytes themselves
+  double *f2b_part_d = nullptr;
+  float *f2b_stats_d = nullptr;
+  unsigned char *bytes_d = nullptr;
+  // streamed output: two pinned staging buffers and their copy events
+  void *stage_h[2] = {nullptr, nullptr};
+  size_t stage_n = 0;
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int *err_d = nullptr;  // [0] abort word of the current launch, [1] sticky report
 };
 
@@ -453,6 +461,10 @@ tr_status tr_destroy(tr_ctx *c) {
   for (auto &kv : c->slots) scratch_free(c, kv.first);
   if (c->hproj_d) cudaFree(c->hproj_d);
   if (c->hvol_d) cudaFree(c->hvol_d);
+  for (int i = 0; i < 2; ++i) {
+    if (c->stage_h[i]) cudaFreeHost(c->stage_h[i]);
+    if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
+  }
   if (c->io_stream) cudaStreamDestroy(c->io_stream);
   if (c->err_d) cudaFree(c->err_d);
   delete c;
@@ -830,34 +842,122 @@ tr_status tr_wbp(tr_ctx *c, float *proj, float *vol, void *stream) {
   return tr_backproject(c, proj, vol, 0, c->th, stream);
 }
 
-tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float *vol_h,
-                              int iters, float gamma) {
-  tr_status st = need_problem(c);
-  if (st) return st;
-  if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
+}  // extern "C"
+
+namespace {
+
+// Uploads the host stack (and the starting volume, or zeroes it) to the
+// context's device copies and runs `method` on them, ordered on io_stream.
+tr_status run_host_method(tr_ctx *c, int method, const float *proj_h, const float *vol_h,
+                          bool zero_start, int iters, float gamma) {
   const size_t pn = proj_elems(c), vn = vol_elems(c);
-  if ((st = host_buffers(c))) return st;
+  tr_status st = host_buffers(c);
+  if (st) return st;
   cudaStream_t s = c->io_stream;
-  const bool zero_start = (method & TR_RECON_ZERO_START) != 0;
-  method &= ~TR_RECON_ZERO_START;
   TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice, s));
   if (zero_start)
     TR_CUDA(c, cudaMemsetAsync(c->hvol_d, 0, vn * sizeof(float), s));
   else
     TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice, s));
   switch (method) {
-    case TR_METHOD_BPT: st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s); break;
-    case TR_METHOD_WBP: st = tr_wbp(c, c->hproj_d, c->hvol_d, s); break;
+    case TR_METHOD_BPT: return tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s);
+    case TR_METHOD_WBP: return tr_wbp(c, c->hproj_d, c->hvol_d, s);
     case TR_METHOD_FBP:
       st = tr_filter_fbp(c, c->hproj_d, 0, s);
-      if (!st) st = tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s);
-      break;
-    case TR_METHOD_SIRT: st = tr_sirt(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
-    case TR_METHOD_SART: st = tr_sart(c, c->hproj_d, c->hvol_d, iters, gamma, s); break;
-    default: st = fail(c, TR_ERR_ARG, "unknown method %d", method);
+      return st ? st : tr_backproject(c, c->hproj_d, c->hvol_d, 0, c->th, s);
+    case TR_METHOD_SIRT: return tr_sirt(c, c->hproj_d, c->hvol_d, iters, gamma, s);
+    case TR_METHOD_SART: return tr_sart(c, c->hproj_d, c->hvol_d, iters, gamma, s);
+    default: return fail(c, TR_ERR_ARG, "unknown method %d", method);
   }
+}
+
+}  // namespace
+
+extern "C" {
+
+tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float *vol_h,
+                              int iters, float gamma) {
+  tr_status st = need_problem(c);
   if (st) return st;
-  TR_CUDA(c, cudaMemcpyAsync(vol_h, c->hvol_d, vn * sizeof(float), cudaMemcpyDeviceToHost, s));
+  if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
+  const bool zero_start = (method & TR_RECON_ZERO_START) != 0;
+  if ((st = run_host_method(c, method & ~TR_RECON_ZERO_START, proj_h, vol_h, zero_start, iters,
+                            gamma)))
+    return st;
+  cudaStream_t s = c->io_stream;
+  TR_CUDA(c, cudaMemcpyAsync(vol_h, c->hvol_d, vol_elems(c) * sizeof(float),
+                             cudaMemcpyDeviceToHost, s));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  return take_timeout(c);
+}
+
+tr_status tr_volume_to_bytes(tr_ctx *c, const float *vol, size_t n, size_t slab, float alpha,
+                             unsigned char *out, void *stream) {
+  if (!c) return TR_ERR_ARG;
+  if (!vol || !out || n == 0 || slab == 0 || (n + slab - 1) / slab > 65535)
+    return fail(c, TR_ERR_ARG, "bad byte-output arguments (n=%zu slab=%zu)", n, slab);
+  TR_CUDA(c, cudaSetDevice(c->device));
+  const size_t nslabs = (n + slab - 1) / slab;
+  tr_status st;
+  if ((st = scratch_alloc(c, (void **)&c->f2b_part_d, nslabs * kF2bParts * sizeof(double),
+                          "byte-output partial sums")) ||
+      (st = scratch_alloc(c, (void **)&c->f2b_stats_d, 4 * nslabs * sizeof(float),
+                          "byte-output statistics")))
+    return st;
+  TR_CUDA(c, launch_f2b(vol, n, slab, alpha, out, c->f2b_part_d, c->f2b_stats_d, c->nsm,
+                        (cudaStream_t)stream));
+  return TR_OK;
+}
+
+tr_status tr_reconstruct_to_sink(tr_ctx *c, int method, const float *proj_h,
+                                 const float *vol_init_h, int iters, float gamma,
+                                 size_t f2b_slab, float f2b_alpha, size_t block_bytes,
+                                 tr_block_sink sink, void *user) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj_h || !sink || block_bytes == 0)
+    return fail(c, TR_ERR_ARG, "bad streamed-output arguments");
+  if ((st = run_host_method(c, method, proj_h, vol_init_h, vol_init_h == nullptr, iters, gamma)))
+    return st;
+  cudaStream_t s = c->io_stream;
+  const size_t vn = vol_elems(c);
+  const unsigned char *src = reinterpret_cast<const unsigned char *>(c->hvol_d);
+  size_t total = vn * sizeof(float);
+  if (f2b_slab) {
+    if ((st = scratch_alloc(c, (void **)&c->bytes_d, vn, "byte volume"))) return st;
+    if ((st = tr_volume_to_bytes(c, c->hvol_d, vn, f2b_slab, f2b_alpha, c->bytes_d, s)))
+      return st;
+    src = c->bytes_d;
+    total = vn;
+  }
+  if (c->stage_n != block_bytes) {
+    for (int i = 0; i < 2; ++i) {
+      if (c->stage_h[i]) cudaFreeHost(c->stage_h[i]);
+      c->stage_h[i] = nullptr;
+    }
+    c->stage_n = 0;
+    for (int i = 0; i < 2; ++i) TR_CUDA(c, cudaHostAlloc(&c->stage_h[i], block_bytes, 0));
+    c->stage_n = block_bytes;
+  }
+  for (int i = 0; i < 2; ++i)
+    if (!c->stage_ev[i])
+      TR_CUDA(c, cudaEventCreateWithFlags(&c->stage_ev[i], cudaEventDisableTiming));
+  const size_t nblocks = (total + block_bytes - 1) / block_bytes;
+  auto issue = [&](size_t k) -> cudaError_t {
+    const size_t off = k * block_bytes, len = std::min(block_bytes, total - off);
+    cudaError_t e = cudaMemcpyAsync(c->stage_h[k & 1], src + off, len, cudaMemcpyDeviceToHost, s);
+    return e == cudaSuccess ? cudaEventRecord(c->stage_ev[k & 1], s) : e;
+  };
+  for (size_t k = 0; k < std::min<size_t>(2, nblocks); ++k) TR_CUDA(c, issue(k));
+  for (size_t k = 0; k < nblocks; ++k) {
+    TR_CUDA(c, cudaEventSynchronize(c->stage_ev[k & 1]));
+    const size_t off = k * block_bytes, len = std::min(block_bytes, total - off);
+    if (sink(user, c->stage_h[k & 1], off, len) != 0) {
+      cudaStreamSynchronize(s);
+      return fail(c, TR_ERR_ARG, "the output sink stopped the transfer at byte %zu", off);
+    }
+    if (k + 2 < nblocks) TR_CUDA(c, issue(k + 2));
+  }
   TR_CUDA(c, cudaStreamSynchronize(s));
   return take_timeout(c);
 }

@@ -258,6 +258,12 @@ cudaError_t admm_p_update(float *p, const float *r, const double *scal, size_t n
                           cudaStream_t s);
 cudaError_t admm_soft(float *u, float *d, const float *x, float soft, size_t n, int nsm,
                       cudaStream_t s);
+// Byte output (tr_output.cu): part[nslabs][kF2bParts] doubles and 4 * nslabs
+// floats of statistics as scratch; nslabs = ceil(n / slab) <= 65535.
+constexpr int kF2bParts = 64;
+cudaError_t launch_f2b(const float *vol, size_t n, size_t slab, float alpha, unsigned char *out,
+                       double *part, float *stats, int nsm, cudaStream_t s);
+
 dim3 bp_tile_grid(const VolView &v);
 dim3 fp_tile_grid(const VolView &v);
 bool batch_bp_layout(const BpArgs &a0, bool sep, size_t budget, BatchBp *out, size_t *smem);

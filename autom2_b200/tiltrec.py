@@ -314,6 +314,17 @@ class Engine:
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")
 
+    def volume_to_bytes(self, vol, slab, alpha=0.9):
+        """tr_volume_to_bytes: a uint8 CUDA tensor of vol's byte mapping."""
+        import torch
+        out = torch.empty(vol.numel(), dtype=torch.uint8, device=vol.device)
+        self.lib.tr_volume_to_bytes.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_size_t,
+                                               C.c_float, C.c_void_p, C.c_void_p]
+        self._check(self.lib.tr_volume_to_bytes(self.h, vol.data_ptr(), vol.numel(), slab,
+                                                alpha, out.data_ptr(), _stream(self.device)),
+                    "tr_volume_to_bytes")
+        return out
+
     def selftest_wait(self, budget_us: int) -> int:
         """tr_selftest_wait's status (TR_ERR_TIMEOUT = -5 when the bounded
         wait gave up, as it should)."""

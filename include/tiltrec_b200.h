@@ -346,6 +346,40 @@ tr_status tr_static_take_timeout(int device);
  * would after a back-projection that gave up. */
 tr_status tr_static_selftest_wait(int device, int budget_us);
 
+/* Byte output of a float volume (--f2b), on the device: for each slab of
+ * `slab` consecutive values (the last may be shorter) its mean and standard
+ * deviation, exponentially averaged over the slabs in order (g = alpha g +
+ * (1 - alpha) stat from g = 0: the Y-layout drivers use alpha 0.9 and 64-row
+ * slabs, the Z-layout ones the whole volume as one slab with alpha 0,
+ * src/TiltRec/src/TiltRec_cuda_z/recon_z.cu:164-172), then every value of
+ * each complete group of four in a slab mapped to
+ * (clamp((v - mean) / std, -10, 10) + 10) / 20 * 255, truncated to a byte
+ * (0 for the values past the last complete group).  Replaces the reference's
+ * per-slab thrust reductions and CufloatToByteKernel
+ * (src/TiltRec/src/TiltRec_cuda_y/recon_y.cu:164-181, basic.cu:442-475);
+ * the slab sums here are FP64 over fixed partitions, so repeated runs give
+ * the same bytes.  vol_dev: n floats; out_dev: n bytes; at most 65535 slabs. */
+tr_status tr_volume_to_bytes(tr_ctx *ctx, const float *vol_dev, size_t n, size_t slab,
+                             float alpha, unsigned char *out_dev, void *stream);
+
+/* Receives consecutive blocks of a reconstruction's output, in order; returns
+ * 0 to continue, non-zero to stop the transfer (the call then fails with
+ * TR_ERR_ARG). */
+typedef int (*tr_block_sink)(void *user, const void *data, size_t offset, size_t bytes);
+
+/* Host-buffer reconstruction whose output streams to the caller in blocks:
+ * as tr_reconstruct_host (vol_init_host NULL: zero start), then, when
+ * f2b_slab > 0, tr_volume_to_bytes on the device with that slab length and
+ * f2b_alpha (the output is then one byte per voxel), and the output is copied
+ * back through two pinned staging buffers of block_bytes each (kept by the
+ * context): the copy of block k+1 is in flight while `sink` consumes block k,
+ * as the reference writes each slab with MrcStackM::WriteBlock while the next
+ * is transferred (src/TiltRec/src/mrcmx/mrcstack.cpp:472-521). */
+tr_status tr_reconstruct_to_sink(tr_ctx *ctx, int method, const float *proj_host,
+                                 const float *vol_init_host, int iters, float gamma,
+                                 size_t f2b_slab, float f2b_alpha, size_t block_bytes,
+                                 tr_block_sink sink, void *user);
+
 /* Area binning of nt images [nt][ny][nx] to [nt][ny/bin][nx/bin] (bin 1..64),
  * the GUI chain's `resample -b bin` before TiltRec (resample/src/main/
  * main.cpp:14-58, OpenCV's area resize): each output pixel is the overlap-

@@ -201,31 +201,38 @@ def test_byte_and_short_stacks(case, restatement):
         compare(d / f"ob{mode}.mrc", d / f"rb{mode}.mrc")
 
 
-def test_f2b_bytes(case):
-    """--f2b: 64-row slabs, EMA mean/deviation (alpha 0.9), z-score clamped
-    to +-10 and mapped to 0..255 (recon_y.cu:164-181, basic.cu:442-475)."""
+@pytest.mark.parametrize("layout", [0, 1])
+def test_f2b_bytes(case, layout):
+    """--f2b, mapped on the device and streamed to the file: Y layout in
+    64-row slabs with EMA mean/deviation (alpha 0.9, recon_y.cu:164-181), Z
+    layout the whole volume with its own statistics (recon_z.cu:164-172);
+    z-score clamped to +-10 and mapped to 0..255 (basic.cu:442-475)."""
     d, proj, ang = case
     common = ["--input", str(d / "stack.mrc"), "--tiltfile", str(d / "a.rawtlt"),
               "--geometry", "0,0,0,8", "--method", "BPT"]
-    ours(0, *common, "--output", str(d / "of.mrc"))
-    ours(0, *common, "--output", str(d / "ob.mrc"), "--f2b")
-    _, _, vol = read_mrc(d / "of.mrc")
-    hb, _, got = read_mrc(d / "ob.mrc")
+    ours(layout, *common, "--output", str(d / f"of{layout}.mrc"))
+    ours(layout, *common, "--output", str(d / f"ob{layout}.mrc"), "--f2b")
+    _, _, vol = read_mrc(d / f"of{layout}.mrc")
+    hb, _, got = read_mrc(d / f"ob{layout}.mrc")
     assert int(hb["mode"]) == 0
     flat = vol.reshape(-1).astype(np.float32)
-    slab = 64 * 8 * 64
+    slab = 64 * 8 * 64 if layout == 0 else flat.size
+    alpha = np.float32(0.9 if layout == 0 else 0.0)
     want = np.zeros(flat.size, np.uint8)
     gm = gs = np.float32(0)
     for s0 in range(0, flat.size, slab):
         c = flat[s0:s0 + slab]
         m = np.float32(c.astype(np.float64).mean())
-        sd = np.float32(np.sqrt(np.float32(((c - m).astype(np.float64) ** 2).mean())))
-        gm = np.float32(0.9) * gm + np.float32(0.1) * m
-        gs = np.float32(0.9) * gs + np.float32(0.1) * sd
+        sd = np.float32(np.sqrt(np.float32(((c - m) ** 2).astype(np.float64).mean())))
+        gm = alpha * gm + (np.float32(1) - alpha) * m
+        gs = alpha * gs + (np.float32(1) - alpha) * sd
         n4 = (c.size // 4) * 4
         z = np.clip((c[:n4] - gm) / gs, -10, 10)
         want[s0:s0 + n4] = (((z + 10) / 20) * 255).astype(np.uint8)
     assert np.mean(np.abs(got.reshape(-1).astype(int) - want.astype(int)) <= 1) > 0.999
+    # header statistics: the middle section of the byte volume
+    mid = got[got.shape[0] // 2].astype(np.float64)
+    assert abs(float(hb["amean"]) - mid.mean()) < 1e-3 * max(1.0, mid.mean())
 
 
 @pytest.mark.parametrize("mode", [2, 1, 0])

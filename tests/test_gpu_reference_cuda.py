@@ -116,3 +116,35 @@ def test_reference_gpu_timing_cfg1_size(engine, tmp_path):
     print(json.dumps({"case": "61 x 1024^2, volume 1024^2 x 256, XTILT 0.3", "runs": times,
                       "sirt_iteration_seconds_ours": it_ours,
                       "sirt_iteration_seconds_reference_gpu": it_ref}))
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_f2b_bytes_vs_reference_gpu_executable(engine, tmp_path, layout):
+    """--f2b: the drop-in's device byte mapping against the reference's own
+    TiltRec-cuda / TiltRecZ-cuda --f2b (CufloatToByteKernel after per-slab
+    thrust reductions; one slab here, the whole 40-row volume) on a WBP
+    without XTILT, where the two float volumes agree to ~1e-6.  The
+    reference's float reductions and ours (FP64) round differently, so a byte
+    may differ by one at a rounding boundary."""
+    ref_exe = O.reference_gpu_executable(layout)
+    if ref_exe is None:
+        pytest.skip("the reference GPU executables were not built")
+    build.build()
+    rng = np.random.default_rng(21 + layout)
+    nt, ny, nx, th = 13, 40, 64, 12
+    ang = np.linspace(-60, 60, nt).astype(np.float32)
+    write_mrc(tmp_path / "stack.mrc", rng.normal(size=(nt, ny, nx)).astype(np.float32))
+    write_angles(tmp_path / "a.tlt", ang)
+    args = ["--input", str(tmp_path / "stack.mrc"), "--tiltfile", str(tmp_path / "a.tlt"),
+            "--geometry", f"0,0,0,{th}", "--method", "WBP", "--f2b"]
+    name = "TiltRec-cuda" if layout == 0 else "TiltRecZ-cuda"
+    ours, _ = _run(os.path.join(BIN, name), args + ["--output", str(tmp_path / "o.mrc")])
+    assert ours.returncode == 0, ours.stderr[-2000:]
+    ref, _ = _run(ref_exe, args + ["--output", str(tmp_path / "r.mrc")])
+    assert ref.returncode == 0, (ref.stdout[-2000:], ref.stderr[-2000:])
+    ho, _, got = read_mrc(tmp_path / "o.mrc")
+    hr, _, want = read_mrc(tmp_path / "r.mrc")
+    assert int(ho["mode"]) == int(hr["mode"]) == 0
+    assert got.shape == want.shape
+    diff = np.abs(got.astype(int) - want.astype(int))
+    assert diff.max() <= 1 and np.mean(diff == 0) > 0.99, (diff.max(), np.mean(diff == 0))
