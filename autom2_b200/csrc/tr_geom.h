@@ -13,10 +13,10 @@ namespace trb {
 
 struct GeomInfo {
   int fw, fh;      // back-projection tile window (columns, rows)
-  int ffw, ffh;    // forward-projection moment window: row stride, rows
-  float nbound;    // most voxel contributions one detector pixel collects
+  int ffw, ffh;    // forward-projection tile window
+  float nbound;    // most voxel contributions one forward window entry collects
   bool sep;        // every tilt has b1 = b3 = 0, b2 = 1 (separable rows)
-  size_t fp_tilt_bytes;  // shared memory of one staged tilt's moment planes
+  size_t fp_tilt_bytes;  // shared memory of one staged tilt's splat window
   size_t bp_tilt_bytes;  // shared memory of one staged tilt's interpolation table
 };
 
@@ -29,11 +29,10 @@ enum GeomStatus {
   GEOM_WINDOW,      // a window side exceeds kMaxWindow
 };
 
-// Most voxels of one forward-projection tile that can add to one detector
-// pixel: along x a row of voxels steps the detector column by |a1|, so at
-// most floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their
-// lower column at q-1 or q; every (y, z) row of the tile may contribute.  A
-// moment entry collects a subset of those voxels.
+// Most voxels of one forward-projection tile that can add to one window entry:
+// along x a row of voxels steps the detector column by |a1|, so at most
+// floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their lower
+// column at q-1 or q; every (y, z) row of the tile may contribute.
 inline float fp_entry_bound(double min_a1) {
   double n = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
   n = std::min(n, (double)kFX);
@@ -84,20 +83,15 @@ inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
   out->fw = (int)std::ceil(span_u) + 4;
   out->fh = sep ? kTY : (int)std::ceil(span_v) + 5;
   // Forward windows start at a 4-column boundary (up to 3 extra columns) and
-  // span whole 4-column groups, so that the flush adds 16-byte groups; each
-  // row has kFPadC zero columns first, and the general form's row stride is
-  // a multiple of kFRowAlign words.  The general form's rows start with one
-  // zero row.
-  const int fcols = ((int)std::ceil(fspan_u) + 4 + 3 + 3) & ~3;
-  const int ralign = sep ? 4 : kFRowAlign;
-  out->ffw = (fcols + kFPadC + ralign - 1) / ralign * ralign;
-  out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5 + 1;
+  // span whole 4-column groups, so that the flush adds 16-byte groups.
+  out->ffw = ((int)std::ceil(fspan_u) + 4 + 3 + 3) & ~3;
+  out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5;
   out->sep = sep;
   out->nbound = fp_entry_bound(min_a1);
-  out->fp_tilt_bytes = (size_t)fp_planes(sep) * out->ffw * out->ffh * sizeof(int);
-  out->bp_tilt_bytes = (size_t)out->fw * out->fh * bp_entry_bytes(sep);
+  out->fp_tilt_bytes = (size_t)out->ffw * out->ffh * sizeof(int);
+  out->bp_tilt_bytes = (size_t)out->fw * out->fh * sizeof(float2);
   if (out->bp_tilt_bytes > smem_max || out->fp_tilt_bytes > smem_max) return GEOM_SMEM;
-  if (std::max(std::max(out->fw, out->fh), std::max(fcols, out->ffh)) > kMaxWindow)
+  if (std::max(std::max(out->fw, out->fh), std::max(out->ffw, out->ffh)) > kMaxWindow)
     return GEOM_WINDOW;
   return GEOM_OK;
 }

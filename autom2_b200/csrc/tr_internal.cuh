@@ -19,18 +19,11 @@ constexpr int kNV = 16;                       // voxels per thread along z
 constexpr int kTZ = kZG * kNV;                // 32
 constexpr int kMaxChunk = 32;                 // tilts staged per chunk (max)
 
-// Forward-projection tile: one x voxel per lane (a warp covers 32 consecutive
-// x), kTY rows and kZG groups of kFNV sections along z, as above.
-constexpr int kFX = kTX;                      // 32
-constexpr int kFNV = 16;                      // voxels per thread along z
+// Forward-projection tile: each lane owns a pair of neighbouring x voxels, so
+// a warp covers 64 x; rows and z groups as above.
+constexpr int kFX = 2 * kTX;                  // 64
+constexpr int kFNV = 16;                      // voxel pairs per thread along z
 constexpr int kFTZ = kZG * kFNV;              // 32
-// Forward-projection moment windows: zero columns before each window row
-// (the flush reads entry column c - 1 for pixel column c), and the row stride
-// of the general form is a multiple of 32 words so that the entries a warp
-// adds to in one instruction (32 consecutive voxels, at most one column apart)
-// fall in distinct banks whatever their rows.
-constexpr int kFPadC = 4;
-constexpr int kFRowAlign = 32;
 
 // Largest tile window side (columns or rows): the kernels step window
 // coordinates in Q9.23 fixed point, whose integer part is below 512.
@@ -100,19 +93,9 @@ struct FpArgs {
   const TiltGeo *geo;
   int t0, nt;
   float ox, oy, oz;
-  int fw, fh, chunk;  // moment window row stride (words, pad included), rows
-                      // (general: one zero row first), tilts per chunk
-  float nbound;       // most voxel contributions one detector pixel can collect
+  int fw, fh, chunk;
+  float nbound;       // most voxel contributions one window entry can collect
 };
-
-// Moment planes of the forward-projection windows: (v, dx v) for separable
-// geometry, (v, dx v, dy v, dx dy v) otherwise.
-constexpr int fp_planes(bool sep) { return sep ? 2 : 4; }
-
-// Bytes of one back-projection table entry: separable geometry interpolates
-// one blended row, (b - s, s); the general form holds both rows of the
-// bilinear step in one entry (see bl_entry in tr_kernels.cu).
-constexpr int bp_entry_bytes(bool sep) { return sep ? 8 : 16; }
 
 // Footprint bookkeeping of one tilt for one tile, computed in FP64.
 struct TileTilt {
@@ -135,8 +118,8 @@ struct WarpStarts {
 };
 
 // Forward-projection coordinate starts of one tilt: the x and z steps and,
-// per warp, U0 + wy A1 + wz kFNV A2 (V likewise); lane l's voxel starts at
-// W + l A0.
+// per warp, U0 + wy A1 + wz kFNV A2 (V likewise); lane l's voxel pair starts
+// at W + 2 l A0.
 struct FpStarts {
   long long A0, A2, B0, B2;
   long long Wu[kThreads / 32], Wv[kThreads / 32];

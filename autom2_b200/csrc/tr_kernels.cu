@@ -21,9 +21,8 @@
 //     UpdateVolumeByProjDiff :492-524): s/c equals bilinear interpolation of
 //     the edge-clamped image whenever the lower neighbour lies in
 //     [-1, nx-1] x [-1, ny-1], and the voxel gets nothing otherwise.  Entries
-//     use the clamped image inside that range and are zero outside it (the
-//     general form's entries are indexed by the lower row, so a lower row
-//     outside [-1, ny-1] finds a zero entry).
+//     use the clamped image inside that range and are zero outside it; rows
+//     below -1 / at or above ny are masked per voxel when a tile can reach them.
 //   * unnormalised gathers (UpdateWeightsByProjDiff :526-562, SIRT): taps
 //     outside the image contribute zero, i.e. interpolation of the zero-padded
 //     image.  Entries use the zero-padded image.
@@ -31,8 +30,7 @@
 // Separable geometry (b1 = b3 = 0, b2 = 1: no XTILT, no in-plane rotation,
 // any per-tilt y shift) interpolates in y with one weight per voxel row, so
 // the two rows are blended while staging and the inner loop is one table
-// read and one FMA per voxel and tilt.  The general form's entry holds both
-// rows of the bilinear step (bl_entry): one 16-byte read and three FMAs.
+// read and one FMA per voxel and tilt.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -47,10 +45,21 @@
 
 namespace trb {
 
+__device__ __forceinline__ float one_plus_frac(unsigned long long U) {
+  // 1 + (low 32 bits / 2^32), truncated to the 23-bit float mantissa.
+  return __uint_as_float(0x3F800000u | ((unsigned)U >> 9));
+}
+
 // Image element -> float.
 __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// Adds the scaled contribution x (|x| <= 2^21) to a fixed-point window entry,
+// rounded to the nearest integer by the 1.5*2^23 float shift.
+__device__ __forceinline__ void wadd(int *p, float x) {
+  atomicAdd(p, __float_as_int(x + 12582912.0f) - 0x4B400000);
+}
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) {
   return v < lo ? lo : (v > hi ? hi : v);
@@ -190,22 +199,6 @@ __device__ __forceinline__ void kahan_add(float &acc, float &c, float val) {
   acc = t;
 }
 
-// Bilinear table entry of the general form for the lower neighbour (k, j):
-// b0, n0 = image(j, k), image(j, k+1); b1, n1 = image(j+1, k), image(j+1, k+1).
-// With the row-j slope s0, the row difference bd = b1 - b0 and its slope sd,
-// row j interpolates to r0 = b0 + dx s0 and the difference to d = bd + dx sd;
-// the entry (r0 - d, d) in the one-FMA form fma(1 + dx, slope, base - slope):
-//   X = fma(F, s0 - sd, (b0 - s0) - (bd - sd)) = r0 - d,
-//   d = fma(F, sd, bd - sd),
-// and the bilinear value is fma(G, d, X) = r0 + dy d with F = 1 + dx,
-// G = 1 + dy.
-__device__ __forceinline__ float4 bl_entry(float b0, float n0, float b1, float n1) {
-  const float s0 = n0 - b0;
-  const float bd = b1 - b0;
-  const float sd = (n1 - b1) - s0;
-  return make_float4((b0 - s0) - (bd - sd), s0 - sd, bd - sd, sd);
-}
-
 // Window coordinates inside the z loop run in Q9.23 (32-bit): the integer
 // part is the window column/row (< 512), the 23 fraction bits are exactly the
 // float mantissa of 1 + dx.  Each thread's start is the exact Q32.32 value
@@ -265,20 +258,35 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
         u += du;
       }
     } else {
-      // One bilinear entry per (lower row, lower column): X = r0 - d and
-      // d = the row difference, both interpolated along x by one FMA each,
-      // then val = X + (1 + dy) d = r0 + dy d (see bl_entry).
       unsigned v = q23((unsigned long long)(st.Wv[w] + lane * st.B0));
       const unsigned dv = st.dv;
-      const float4 *T = reinterpret_cast<const float4 *>(tblv) + (size_t)i * per;
+      const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)i * per;
+      const int jmin = st.jmin;
+      if (MODE == BP_NORM && st.check_rows) {
 #pragma unroll
-      for (int k = 0; k < kNV; ++k) {
-        const float4 t = T[(int)(v >> 23) * fw + (int)(u >> 23)];
-        const float F = one_plus_frac23(u);
-        const float X = fmaf(F, t.y, t.x), d = fmaf(F, t.w, t.z);
-        sum[k] += fmaf(one_plus_frac23(v), d, X);
-        u += du;
-        v += dv;
+        for (int k = 0; k < kNV; ++k) {
+          const int q = (int)(u >> 23), r = (int)(v >> 23);
+          const float2 *e = T + r * fw + q;
+          const float2 t0 = e[0], t1 = e[fw];
+          const float f = one_plus_frac23(u);
+          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
+          const float val = fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
+          if ((unsigned)(jmin + r + 1) <= (unsigned)pny) sum[k] += val;
+          u += du;
+          v += dv;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < kNV; ++k) {
+          const int q = (int)(u >> 23), r = (int)(v >> 23);
+          const float2 *e = T + r * fw + q;
+          const float2 t0 = e[0], t1 = e[fw];
+          const float f = one_plus_frac23(u);
+          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
+          sum[k] += fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
+          u += du;
+          v += dv;
+        }
       }
     }
   }
@@ -316,8 +324,7 @@ __global__ void __launch_bounds__(kThreads)
     bp_kernel(const BpArgs a) {
   constexpr bool KAHAN = !std::is_same<IT, float>::value;
   extern __shared__ float4 tbl_raw[];
-  float2 *tbl2 = reinterpret_cast<float2 *>(tbl_raw);  // separable: (b - s, s)
-  float4 *tbl4 = tbl_raw;                              // general: bl_entry
+  float2 *tbl2 = reinterpret_cast<float2 *>(tbl_raw);
   __shared__ TileTilt tt[kMaxChunk];
   __shared__ SepW sw[kMaxChunk][kTY];
   __shared__ WarpStarts ws[kMaxChunk];
@@ -364,18 +371,13 @@ __global__ void __launch_bounds__(kThreads)
         const float sl = n - b;
         tbl2[e] = make_float2(b - sl, sl);
       } else {
-        // Lower row j: normalised gathers take the clamped image for lower
-        // neighbours in [-1, nx-1] x [-1, ny-1] and nothing otherwise.
         const int j = tt[i].jmin + r;
         const bool valid = (MODE != BP_NORM) ||
-                           (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny - 1);
-        float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid)
-          t = bl_entry(img_at<MODE>(p, sc, pnx, pny, j, x0),
-                       img_at<MODE>(p, sc, pnx, pny, j, x0 + 1),
-                       img_at<MODE>(p, sc, pnx, pny, j + 1, x0),
-                       img_at<MODE>(p, sc, pnx, pny, j + 1, x0 + 1));
-        tbl4[e] = t;
+                           (x0 >= -1 && x0 <= pnx - 1 && j >= -1 && j <= pny);
+        const float b = valid ? img_at<MODE>(p, sc, pnx, pny, j, x0) : 0.f;
+        const float n = valid ? img_at<MODE>(p, sc, pnx, pny, j, x0 + 1) : 0.f;
+        const float sl = n - b;
+        tbl2[e] = make_float2(b - sl, sl);
       }
     }
     __syncthreads();
@@ -513,12 +515,10 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
   TileTilt *tt = reinterpret_cast<TileTilt *>(dsm);
   SepW(*sw)[kTY] = reinterpret_cast<SepW(*)[kTY]>(dsm + (size_t)nt * sizeof(TileTilt));
   IT *raw0 = reinterpret_cast<IT *>(dsm + a.tma_raw_offset);
-  float *tblf = reinterpret_cast<float *>(raw0 + 2 * (size_t)chunk * rs);  // table entries
-  WarpStarts *ws = reinterpret_cast<WarpStarts *>(tblf + (bp_entry_bytes(SEP) / 4) *
-                                                            (size_t)chunk * per);
+  float *tblf = reinterpret_cast<float *>(raw0 + 2 * (size_t)chunk * rs);  // float2 entries
+  WarpStarts *ws = reinterpret_cast<WarpStarts *>(tblf + 2 * (size_t)chunk * per);
   constexpr int kXAlign = 16 / (int)sizeof(IT);  // TMA x coordinates: 16-byte multiples
-  float2 *tbl2 = reinterpret_cast<float2 *>(tblf);  // separable entries
-  float4 *tbl4 = reinterpret_cast<float4 *>(tblf);  // general entries (bl_entry)
+  float2 *tbl2 = reinterpret_cast<float2 *>(tblf);
 
   for (int i = tid; i < nt; i += kThreads) {
     tile_setup(a.geo[a.t0 + i], xc, yc, zc, a.ox, a.oy, a.oz, pny, SEP, kTX - 1, kTY - 1,
@@ -631,39 +631,31 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
       // group index g in the chunk's tables.
       auto stage = [&](int i, int r, int q, int g) {
         const IT *R = R0 + (size_t)i * rs;  // raw column = table column
-        float p0[5], p1[5];  // rows r and r + 1 (in the raw box for any r < fh)
-        if (MODE != BP_NORM) {
-          load5(R + r * bw + q, p0);
-          load5(R + (r + 1) * bw + q, p1);
-        }
+        float p[5];
+        if (MODE != BP_NORM) load5(R + r * bw + q, p);  // in the raw box for any r < fh
         const TileTilt &t = tt[c0 + i];
         if (r >= t.nr || q >= t.nq) return;
         const float sc = a.img.scale ? a.img.scale[a.t0 + c0 + i] : 1.f;
         const int xs = t.kmin, ys = t.jmin;
         const int x0 = xs + q;  // image column of the group's first entry
-        const int j = ys + r;   // its lower image row
-        if (MODE != BP_NORM || (x0 >= 0 && x0 + 4 <= pnx - 1 && j >= 0 && j + 1 <= pny - 1)) {
-          if (MODE == BP_NORM) {
-            load5(R + r * bw + q, p0);
-            load5(R + (r + 1) * bw + q, p1);
-          }
-          float4 *d = tbl4 + (size_t)g * 4;
+        const int j = ys + r;
+        if (MODE != BP_NORM || (x0 >= 0 && x0 + 4 <= pnx - 1 && j >= 0 && j <= pny - 1)) {
+          if (MODE == BP_NORM) load5(R + r * bw + q, p);
 #pragma unroll
-          for (int m = 0; m < 4; ++m)
-            d[m] = bl_entry(p0[m] * sc, p0[m + 1] * sc, p1[m] * sc, p1[m + 1] * sc);
+          for (int m = 0; m < 5; ++m) p[m] *= sc;
+          store_group(tbl2 + (size_t)g * 4, p);
         } else {  // border: per entry, clamped; zero outside the valid range
-          const IT *row0 = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
-          const IT *row1 = R + (clampi(j + 1, 0, pny - 1) - ys) * bw - xs;
+          const IT *row = R + (clampi(j, 0, pny - 1) - ys) * bw - xs;
 #pragma unroll
           for (int m = 0; m < 4; ++m) {
             const int x = x0 + m;
-            float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (x >= -1 && x <= pnx - 1 && j >= -1 && j <= pny - 1) {
-              const int kb = clampi(x, 0, pnx - 1), kn = clampi(x + 1, 0, pnx - 1);
-              e = bl_entry(to_f(row0[kb]) * sc, to_f(row0[kn]) * sc, to_f(row1[kb]) * sc,
-                           to_f(row1[kn]) * sc);
+            float b = 0.f, n = 0.f;
+            if (x >= -1 && x <= pnx - 1 && j >= -1 && j <= pny) {
+              b = to_f(row[clampi(x, 0, pnx - 1)]) * sc;
+              n = to_f(row[clampi(x + 1, 0, pnx - 1)]) * sc;
             }
-            tbl4[(size_t)g * 4 + m] = e;
+            const float sl = n - b;
+            tbl2[(size_t)g * 4 + m] = make_float2(b - sl, sl);
           }
         }
       };
@@ -711,48 +703,34 @@ __global__ void __launch_bounds__(kThreads, 4)
 }
 
 // Forward projection: voxel splat (Reproject, main/main-mpi.cpp:286-344) of
-// one tile into per-tilt shared-memory windows, then one global reduction per
-// group of four touched in-image detector pixels.  v.vol == nullptr splats
-// ones (the per-pixel weight sums, reproj_wt).
+// one tile into per-tilt shared-memory windows, then one global atomic add per
+// touched in-image detector pixel.  v.vol == nullptr splats ones (the
+// per-pixel weight sums, reproj_wt).
 //
-// Moment form.  A voxel of value v whose detector coordinate is (u, w), with
-// lower neighbour (q, r) = (floor u, floor w) and fractions (dx, dy), adds
-// (1-dx)(1-dy)v, dx(1-dy)v, (1-dx)dy v and dx dy v to pixels (q, r),
-// (q+1, r), (q, r+1), (q+1, r+1).  Instead, it adds the four moments
-//   M00 = v,  M10 = dx v,  M01 = dy v,  M11 = dx dy v
-// to entry (q, r) of four planes, and the flush forms each pixel from the
-// moments of the entries that reach it:
-//   P(q, r) = [M00 - M10 - M01 + M11](q, r) + [M10 - M11](q-1, r)
-//           + [M01 - M11](q, r-1) + M11(q-1, r-1).
-// Separable geometry (one detector row per voxel row, split at the flush)
-// needs M00 and M10 only: P(q) = [M00 - M10](q) + M10(q-1).
+// Each lane owns the voxel pair (x, x+1) with x = xc + 2*lane and splats
+// the two voxels in turn: lanes of one atomic instruction are then two voxels
+// apart along x and land on distinct detector columns whenever |a1| >= 0.5.
 //
-// Fixed point.  The tile's values are scaled by a power of two S chosen from
-// its largest |voxel| so that no entry or pixel sum can overflow 2^30 (a pixel
-// collects at most `nbound` voxels, host bound from the x slope) and every
-// moment stays below 2^22; each voxel is rounded once to an integer v_int
-// (M00), and each other moment is rounded to the nearest integer by a float
-// shift: fma(1+dx, v, 1.5*2^23 - v) = 1.5*2^23 + dx*v, whose low bits are the
-// rounded product.  The window sums are exact integer sums (order-independent;
-// shared-memory integer atomics are native, float ones are a compare-and-swap
-// loop), and the pixel combination is exact in 32-bit wrap-around arithmetic.
-//
-// Lanes own consecutive x voxels, so the entries one atomic instruction adds
-// to lie within 32 consecutive columns (|a1| <= 1), and with the general
-// form's row stride a multiple of 32 words they fall in distinct banks
-// whichever row each lane is on (lanes on the same entry add to one address).
-
+// The windows accumulate in 32-bit fixed point with native shared-memory
+// integer atomics (fire-and-forget; float atomics on shared memory are a
+// compare-and-swap loop whose round trips left the kernel latency-bound).  The
+// tile's values are scaled by a power of two S chosen from the tile's largest
+// |voxel| so that no window entry can overflow: an entry collects at most
+// `nbound` voxel contributions (host bound from the x slope) of magnitude at
+// most max|v|, and S <= 2^30 / (nbound max|v|); also S <= 2^20 / max|v| so a
+// voxel pair's combined contribution stays within the exact range of the
+// float-shift rounding (|x| < 2^22).  Each contribution is rounded
+// to the nearest integer of its scaled value (a quantum of
+// nbound * max|v| * 2^-30, ~1e-9 of the tile's largest value for tilts
+// within +-60 degrees); the sums are exact and independent of atomic order.
+// The flush converts back (x 1/S) and adds the in-image pixels to the global
+// float accumulators.
 // Adds four floats to four consecutive global floats (16-byte aligned).
 __device__ __forceinline__ void red_add_v4(float *p, float x, float y, float z, float w) {
   asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(__cvta_generic_to_global(p)),
                "f"(x), "f"(y), "f"(z), "f"(w)
                : "memory");
 }
-
-// Float shift that rounds to an integer: bits(x + kShift) = kShiftBits + round(x)
-// for |x| < 2^22.
-constexpr float kShift = 12582912.0f;  // 1.5 * 2^23
-constexpr int kShiftBits = 0x4B400000;
 
 // A forward-projection CTA's shared bookkeeping.  Declared once per kernel and
 // passed in, so that a kernel instantiating both fp_tile forms holds one copy.
@@ -767,7 +745,7 @@ struct FpShared {
 
 template <bool SEP>
 __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
-                                        int *win, FpShared &sh) {
+                                        float *accs, FpShared &sh) {
   TileTilt *const tt = sh.tt;
   SepW(*const sw)[kTY] = sh.sw;
   FpStarts *const fs = sh.fs;
@@ -778,56 +756,60 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
   // 16-byte pixel groups of the stack: rows and tilt planes of whole groups.
   const bool vec_ok = ((a.pnx | (int)a.tstride) & 3) == 0 &&
                       (reinterpret_cast<uintptr_t>(a.val) & 15) == 0;
-  const int wy = warp % kTY;
-  const int wz = warp / kTY;
+  const int wy = (tid >> 5) % kTY;
+  const int wz = (tid >> 5) / kTY;
   const int xc = bx * kFX, yc = by * kTY, zl = bz * kFTZ;
   const int zc = zl + a.v.zoff;
-  const int fw = a.fw, fh = a.fh;
-  const int per = fh * fw;         // words of one tilt's plane
-  const int PS = a.chunk * per;    // words between planes
+  const int fw = a.fw, fh = SEP ? kTY : a.fh;
+  const int per = fh * fw;
 
-  float vf[kFNV];  // scaled voxel values, rounded to integers
-  int vi[kFNV];    // the same as ints (M00)
+  float va[kFNV], vb[kFNV];
   {
-    const int x = xc + lane, y = yc + wy;
-    const bool in = x < a.v.nx && y < a.v.ny;
+    const int x = xc + 2 * lane, y = yc + wy;
+    const bool ina = x < a.v.nx && y < a.v.ny, inb = x + 1 < a.v.nx && y < a.v.ny;
 #pragma unroll
     for (int k = 0; k < kFNV; ++k) {
       const int z = zl + wz * kFNV + k;
       const float *p = a.v.vol + (size_t)y * a.v.sy + (size_t)z * a.v.sz + x;
-      vf[k] = !(in && z < a.v.nz) ? 0.f : (a.v.vol ? __ldg(p) : 1.f);
+      const bool inz = z < a.v.nz;
+      va[k] = !(ina && inz) ? 0.f : (a.v.vol ? __ldg(p) : 1.f);
+      vb[k] = !(inb && inz) ? 0.f : (a.v.vol ? __ldg(p + 1) : 1.f);
     }
   }
   // Tile scale: largest |v| over the tile (as ordered float bits).
+  unsigned *const wmax = sh.wmax;
+  float &s_scale = sh.scale, &s_inv = sh.inv;
+  int &s_nonzero = sh.nonzero;
   {
     unsigned m = 0;
 #pragma unroll
-    for (int k = 0; k < kFNV; ++k) m = max(m, __float_as_uint(fabsf(vf[k])));
+    for (int k = 0; k < kFNV; ++k)
+      m = max(m, max(__float_as_uint(fabsf(va[k])), __float_as_uint(fabsf(vb[k]))));
     m = __reduce_max_sync(0xffffffffu, m);
-    if (lane == 0) sh.wmax[warp] = m;
+    if (lane == 0) wmax[tid >> 5] = m;
     __syncthreads();
     if (tid == 0) {
       unsigned mm = 0;
-      for (int w = 0; w < kThreads / 32; ++w) mm = max(mm, sh.wmax[w]);
+      for (int w = 0; w < kThreads / 32; ++w) mm = max(mm, wmax[w]);
       const float vmax = __uint_as_float(mm);
-      const float lim = vmax > 0.f ? fminf(1073741824.0f / (a.nbound * vmax), 1048576.0f / vmax)
-                                   : 1.f;
+      float lim = vmax > 0.f ? fminf(1073741824.0f / (a.nbound * vmax), 1048576.0f / vmax)
+                             : 1.f;
       int ex;
       frexpf(lim, &ex);  // lim = m 2^ex, m in [0.5, 1): 2^(ex-1) <= lim
-      sh.scale = ldexpf(1.f, ex - 1);
-      sh.inv = ldexpf(1.f, 1 - ex);
-      sh.nonzero = vmax > 0.f;
+      s_scale = ldexpf(1.f, ex - 1);
+      s_inv = ldexpf(1.f, 1 - ex);
+      s_nonzero = vmax > 0.f;
     }
     __syncthreads();
-    const float S = sh.scale;
+    const float S = s_scale;
 #pragma unroll
     for (int k = 0; k < kFNV; ++k) {
-      const float r = vf[k] * S + kShift;  // rounds v S to an integer
-      vi[k] = __float_as_int(r) - kShiftBits;
-      vf[k] = r - kShift;
+      va[k] *= S;
+      vb[k] *= S;
     }
   }
-  const bool nonzero = sh.nonzero != 0;  // an all-zero tile adds nothing
+  int *const iacc = reinterpret_cast<int *>(accs);
+  const bool s_scale_nonzero = s_nonzero != 0;  // an all-zero tile adds nothing
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
@@ -852,106 +834,98 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
         st.Wv[w] = tt[tid].V0 + ry * g.B[1] + (long long)(rz * kFNV) * g.B[2];
       }
     }
-    {
-      int4 *w4 = reinterpret_cast<int4 *>(win);
-      const int n4 = (fp_planes(SEP) * PS) >> 2;
-      for (int e = tid; e < n4; e += kThreads) w4[e] = make_int4(0, 0, 0, 0);
-    }
+    for (int e = tid; e < nc * per; e += kThreads) iacc[e] = 0;
     __syncthreads();
 
-    for (int i = 0; i < nc && nonzero; ++i) {
+    for (int i = 0; i < nc && s_scale_nonzero; ++i) {
       const FpStarts &st = fs[i];
-      unsigned u = q23((unsigned long long)(st.Wu[warp] + lane * st.A0));
-      const unsigned du = q23_step(st.A2);
+      const long long A0 = st.A0, A2 = st.A2;
+      // Lane coordinates of the pair's voxels: A at x = xc + 2 lane, B at x+1.
+      unsigned long long UA = (unsigned long long)(st.Wu[warp] + (2 * lane) * A0);
+      unsigned long long UB = UA + (unsigned long long)A0;
       if (SEP) {
-        int *M0 = win + i * per + wy * fw + kFPadC;
-        int *M1 = M0 + PS;
+        int *T = iacc + (size_t)(i * kTY + wy) * fw;
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
-          const int q = (int)(u >> 23);
-          const float F = one_plus_frac23(u);
-          const int m10 = __float_as_int(fmaf(F, vf[k], kShift - vf[k])) - kShiftBits;
-          atomicAdd(M0 + q, vi[k]);
-          atomicAdd(M1 + q, m10);
-          u += du;
+          // dx*v as one rounding of (1+dx)*v - v; the pair's lanes are two x
+          // apart, so one instruction's lanes hit distinct columns.
+          const float vA = va[k], vB = vb[k];
+          const float t1a = fmaf(one_plus_frac(UA), vA, -vA), t0a = vA - t1a;
+          const float t1b = fmaf(one_plus_frac(UB), vB, -vB), t0b = vB - t1b;
+          int *ea = T + (int)(UA >> 32), *eb = T + (int)(UB >> 32);
+          wadd(ea, t0a);
+          wadd(ea + 1, t1a);
+          wadd(eb, t0b);
+          wadd(eb + 1, t1b);
+          UA += (unsigned long long)A2;
+          UB += (unsigned long long)A2;
         }
       } else {
-        unsigned v = q23((unsigned long long)(st.Wv[warp] + lane * st.B0));
-        const unsigned dv = q23_step(st.B2);
-        int *M00 = win + i * per + fw + kFPadC;  // row 0 of the window is zero
+        const long long B0 = st.B0, B2 = st.B2;
+        unsigned long long VA = (unsigned long long)(st.Wv[warp] + (2 * lane) * B0);
+        unsigned long long VB = VA + (unsigned long long)B0;
+        int *T = iacc + (size_t)i * per;
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
-          const int e = (int)(v >> 23) * fw + (int)(u >> 23);
-          const float F = one_plus_frac23(u), G = one_plus_frac23(v);
-          const float cv = kShift - vf[k];
-          const int m10 = __float_as_int(fmaf(F, vf[k], cv)) - kShiftBits;
-          const float y1 = fmaf(G, vf[k], cv);  // kShift + round(dy v)
-          const float m01f = y1 - kShift;       // round(dy v), exact
-          const int m11 = __float_as_int(fmaf(F, m01f, kShift - m01f)) - kShiftBits;
-          atomicAdd(M00 + e, vi[k]);
-          atomicAdd(M00 + PS + e, m10);
-          atomicAdd(M00 + 2 * PS + e, __float_as_int(y1) - kShiftBits);
-          atomicAdd(M00 + 3 * PS + e, m11);
-          u += du;
-          v += dv;
+          const float vA = va[k], vB = vb[k];
+          {
+            const float y1 = fmaf(one_plus_frac(VA), vA, -vA), y0 = vA - y1;
+            const float fx = one_plus_frac(UA);
+            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
+            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            int *e = T + (int)(VA >> 32) * fw + (int)(UA >> 32);
+            wadd(e, t00);
+            wadd(e + 1, t01);
+            wadd(e + fw, t10);
+            wadd(e + fw + 1, t11);
+          }
+          {
+            const float y1 = fmaf(one_plus_frac(VB), vB, -vB), y0 = vB - y1;
+            const float fx = one_plus_frac(UB);
+            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
+            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            int *e = T + (int)(VB >> 32) * fw + (int)(UB >> 32);
+            wadd(e, t00);
+            wadd(e + 1, t01);
+            wadd(e + fw, t10);
+            wadd(e + fw + 1, t11);
+          }
+          UA += (unsigned long long)A2;
+          UB += (unsigned long long)A2;
+          VA += (unsigned long long)B2;
+          VB += (unsigned long long)B2;
         }
       }
     }
     __syncthreads();
 
-    // Flush: pixels from the moments, in-image pixels only, as the
-    // reference's splat.  Four columns per thread: a group inside the image
-    // goes out as one 16-byte vector reduction when the stack's rows are
-    // 16-byte aligned; border groups add their in-image pixels one by one.
+    // Flush the windows: in-image pixels only, as the reference's splat.
+    // Four columns per thread: a group inside the image goes out as one
+    // 16-byte vector reduction when the stack's rows are 16-byte aligned;
+    // border groups add their in-image pixels one by one.
     for (int i = 0; i < nc; ++i) {
-      const int kmin = tt[i].kmin, nq = tt[i].nq;
-      const int nr = SEP ? kTY : tt[i].nr;
+      const int kmin = tt[i].kmin, nq = tt[i].nq, nr = tt[i].nr;
+      const int *T = iacc + (size_t)i * per;
       float *base = a.val + (size_t)(a.t0 + c0 + i) * a.tstride;
-      const float inv = sh.inv;
+      const float inv = s_inv;
       const int ngq = (nq + 3) >> 2;
       for (int e = tid; e < nr * ngq; e += kThreads) {
         const int r = e / ngq, q = (e - r * ngq) << 2;
-        int p[4];
-        if (SEP) {
-          const int *M0 = win + i * per + r * fw + kFPadC + q;
-          const int *M1 = M0 + PS;
-          const int4 a0 = *reinterpret_cast<const int4 *>(M0);
-          const int4 a1 = *reinterpret_cast<const int4 *>(M1);
-          const int l1 = M1[-1];
-          p[0] = a0.x - a1.x + l1;
-          p[1] = a0.y - a1.y + a1.x;
-          p[2] = a0.z - a1.z + a1.y;
-          p[3] = a0.w - a1.w + a1.z;
-        } else {
-          const int *R = win + i * per + (r + 1) * fw + kFPadC + q;  // entry row r
-          const int4 m00 = *reinterpret_cast<const int4 *>(R);
-          const int4 m10 = *reinterpret_cast<const int4 *>(R + PS);
-          const int4 m01 = *reinterpret_cast<const int4 *>(R + 2 * PS);
-          const int4 m11 = *reinterpret_cast<const int4 *>(R + 3 * PS);
-          const int4 u01 = *reinterpret_cast<const int4 *>(R + 2 * PS - fw);  // row r-1
-          const int4 u11 = *reinterpret_cast<const int4 *>(R + 3 * PS - fw);
-          const int l10 = R[PS - 1], l11 = R[3 * PS - 1], ul11 = R[3 * PS - fw - 1];
-          // [M00 - M10 - M01 + M11](q) + [M10 - M11](q-1) + [M01 - M11](q, r-1)
-          // + M11(q-1, r-1)
-          p[0] = m00.x - m10.x - m01.x + m11.x + l10 - l11 + u01.x - u11.x + ul11;
-          p[1] = m00.y - m10.y - m01.y + m11.y + m10.x - m11.x + u01.y - u11.y + u11.x;
-          p[2] = m00.z - m10.z - m01.z + m11.z + m10.y - m11.y + u01.z - u11.z + u11.y;
-          p[3] = m00.w - m10.w - m01.w + m11.w + m10.z - m11.z + u01.w - u11.w + u11.z;
-        }
-        if ((p[0] | p[1] | p[2] | p[3]) == 0) continue;
-        const float s[4] = {(float)p[0] * inv, (float)p[1] * inv, (float)p[2] * inv,
-                            (float)p[3] * inv};
+        const int4 v = *reinterpret_cast<const int4 *>(T + r * fw + q);
+        const float s[4] = {(float)v.x * inv, (float)v.y * inv, (float)v.z * inv,
+                            (float)v.w * inv};
+        if (s[0] == 0.f && s[1] == 0.f && s[2] == 0.f && s[3] == 0.f) continue;
         const int k = kmin + q;
         const bool inside = vec_ok && k >= 0 && k + 3 < a.pnx;
         auto add_row = [&](int j, float wgt) {
           if ((unsigned)j >= (unsigned)a.pny) return;
-          float *pp = base + (size_t)j * a.pnx + k;
-          if (inside && (reinterpret_cast<uintptr_t>(pp) & 15) == 0) {
-            red_add_v4(pp, s[0] * wgt, s[1] * wgt, s[2] * wgt, s[3] * wgt);
+          float *p = base + (size_t)j * a.pnx + k;
+          if (inside && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+            red_add_v4(p, s[0] * wgt, s[1] * wgt, s[2] * wgt, s[3] * wgt);
           } else {
 #pragma unroll
             for (int m = 0; m < 4; ++m)
-              if (s[m] != 0.f && (unsigned)(k + m) < (unsigned)a.pnx) atomicAdd(pp + m, s[m] * wgt);
+              if (s[m] != 0.f && (unsigned)(k + m) < (unsigned)a.pnx) atomicAdd(p + m, s[m] * wgt);
           }
         };
         if (SEP) {
@@ -969,10 +943,10 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
 }
 
 template <bool SEP>
-__global__ void __launch_bounds__(kThreads, 3) fp_kernel(const FpArgs a) {
-  extern __shared__ __align__(16) int win[];
+__global__ void __launch_bounds__(kThreads, SEP ? 3 : 4) fp_kernel(const FpArgs a) {
+  extern __shared__ __align__(16) float accs[];
   __shared__ FpShared sh;
-  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, win, sh);
+  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs, sh);
 }
 
 // SIRT residual (main/main-mpi.cpp:640-647): r = p - (wt != 0 ? val/wt : val),
@@ -1202,8 +1176,8 @@ __global__ void quantize_batch_kernel(const BatchTable *T) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads, 3) fp_batch_kernel(BatchTable *T) {
-  extern __shared__ __align__(16) int win[];
+__global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
+  extern __shared__ __align__(16) float accs[];
   __shared__ long long s_tile;
   __shared__ int s_item;
   __shared__ FpShared sh;
@@ -1224,8 +1198,8 @@ __global__ void __launch_bounds__(kThreads, 3) fp_batch_kernel(BatchTable *T) {
     const int bx = (int)(l % it.gx);
     l /= it.gx;
     const int by = (int)(l % it.gy), bz = (int)(l / it.gy);
-    if (it.sep) fp_tile<true>(it.a, bx, by, bz, win, sh);
-    else fp_tile<false>(it.a, bx, by, bz, win, sh);
+    if (it.sep) fp_tile<true>(it.a, bx, by, bz, accs, sh);
+    else fp_tile<false>(it.a, bx, by, bz, accs, sh);
   }
 }
 
@@ -1277,7 +1251,7 @@ static dim3 tile_grid(const VolView &v) {
 template <int MODE, bool SEP, typename IT>
 static cudaError_t launch_bp_t(const BpArgs &a, cudaStream_t s) {
   const int fh = SEP ? kTY : a.fh;
-  const size_t smem = (size_t)a.chunk * fh * a.fw * bp_entry_bytes(SEP);
+  const size_t smem = (size_t)a.chunk * fh * a.fw * sizeof(float2);
   cudaError_t e = cudaFuncSetAttribute(
       bp_kernel<MODE, SEP, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
       (int)smem);
@@ -1341,7 +1315,7 @@ static bool tma_layout(const BpArgs &a0, bool sep, size_t budget, BpArgs *out,
   const size_t fixed =
       ((size_t)a0.nt * (sizeof(TileTilt) + kTY * sizeof(SepW)) + 127) & ~(size_t)127;
   const size_t per_tilt =
-      2 * (size_t)rs * es + (size_t)fh * fwt * bp_entry_bytes(sep) + sizeof(WarpStarts);
+      2 * (size_t)rs * es + (size_t)fh * fwt * sizeof(float2) + sizeof(WarpStarts);
   if (fixed + per_tilt > budget + 64 * 1024) return false;
   int chunk = (int)std::max<size_t>(1, (budget > fixed ? budget - fixed : 0) / per_tilt);
   chunk = std::min(chunk, std::min(kMaxChunk, a0.nt));
@@ -1420,7 +1394,8 @@ static dim3 fp_grid(const VolView &v) {
 }
 
 cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s) {
-  const size_t smem = (size_t)fp_planes(sep) * a.chunk * a.fh * a.fw * sizeof(int);
+  const int fh = sep ? kTY : a.fh;
+  const size_t smem = (size_t)a.chunk * fh * a.fw * sizeof(float);
   cudaError_t e;
   if (sep) {
     e = cudaFuncSetAttribute(fp_kernel<true>,
