@@ -55,7 +55,14 @@ struct tr_ctx {
   std::map<void **, Slot> slots;
   unsigned gen = 0;
   size_t scratch = 0;
-  float *val_d = nullptr, *wt_d = nullptr, *wtvol_d = nullptr;
+  float *val_d = nullptr, *wt_d = nullptr;
+  // SIRT voxel weights in compact form (BpArgs::wslot): a slot per tile of
+  // the view [w_z0, w_z0 + w_nz), the border tiles' weights, the separable
+  // per-row weights
+  float *wtvol_d = nullptr, *wrow_d = nullptr;
+  int *wslot_d = nullptr;
+  int w_z0 = -1, w_nz = -1;
+  long long w_border = 0;
   void *res16_d = nullptr;      // 16-bit SIRT residual [ntilt][ny][nx]
   unsigned *maxbits_d = nullptr;  // per-tilt |p| maxima for tr_quantize
   float *rscale_d = nullptr;      // per-tilt scales of the FP16 SIRT residual
@@ -184,7 +191,7 @@ VolView full_view(const tr_ctx *c, float *vol, int z0, int nz) {
 
 BpArgs bp_args(const tr_ctx *c, float *vol, int z0, int nz, const float *img,
                int t0, int nt, float gamma) {
-  BpArgs a;
+  BpArgs a{};
   a.v = full_view(c, vol, z0, nz);
   a.img.p = img;
   a.img.nx = c->nx;
@@ -359,17 +366,58 @@ tr_status ensure_wt(tr_ctx *c, cudaStream_t s) {
   return TR_OK;
 }
 
-tr_status ensure_wtvol(tr_ctx *c, cudaStream_t s) {
-  tr_status st = scratch_alloc(c, (void **)&c->wtvol_d, vol_elems(c) * sizeof(float),
-                               "voxel weights");
-  if (st) return st;
-  if (!c->wtvol_ready) {
-    BpArgs a = bp_args(c, c->wtvol_d, 0, c->th, nullptr, 0, c->nt, 1.f);
-    a.out = c->wtvol_d;
-    TR_CUDA(c, run_bp(c, BP_WEIGHTS, a, s));
-    c->wtvol_ready = true;
+// SIRT voxel weights of sections [z0, z0 + nz), compact: the view's tiles are
+// classified on the device (one read of the border count), the border tiles'
+// weights computed by the weight pass, interior ones implied (BpArgs::wslot).
+tr_status ensure_wtvol(tr_ctx *c, int z0, int nz, cudaStream_t s) {
+  if (c->wtvol_ready && c->w_z0 == z0 && c->w_nz == nz) {
+    c->slots[(void **)&c->wtvol_d].gen = c->slots[(void **)&c->wslot_d].gen = c->gen;
+    if (c->wrow_d) c->slots[(void **)&c->wrow_d].gen = c->gen;
+    return TR_OK;
   }
+  c->wtvol_ready = false;
+  const VolView v = full_view(c, nullptr, z0, nz);
+  const dim3 g = bp_tile_grid(v);
+  const size_t ntiles = (size_t)g.x * g.y * g.z;
+  tr_status st = scratch_alloc(c, (void **)&c->wslot_d, (ntiles + 1) * sizeof(int),
+                               "voxel-weight tile slots");
+  if (st) return st;
+  int *count = c->wslot_d + ntiles;
+  TR_CUDA(c, cudaMemsetAsync(count, 0, sizeof(int), s));
+  TR_CUDA(c, launch_classify_tiles(c->geo_d, c->nt, v, c->ox, c->oy, c->oz, c->nx, c->ny, c->sep,
+                                   c->wslot_d, count, s));
+  int nborder = 0;
+  TR_CUDA(c, cudaMemcpyAsync(&nborder, count, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  if ((st = scratch_alloc(c, (void **)&c->wtvol_d,
+                          std::max<size_t>(1, (size_t)nborder) * kTileVox * sizeof(float),
+                          "border-tile voxel weights")))
+    return st;
+  if (c->sep) {
+    if ((st = scratch_alloc(c, (void **)&c->wrow_d, (size_t)c->ny * sizeof(float),
+                            "row voxel weights")))
+      return st;
+    TR_CUDA(c, launch_sep_row_weights(c->geo_d, c->nt, c->ny, c->oy, c->ny, c->wrow_d, s));
+  }
+  if (nborder > 0) {
+    BpArgs a = bp_args(c, nullptr, z0, nz, nullptr, 0, c->nt, 1.f);
+    a.out = c->wtvol_d;
+    a.wslot = c->wslot_d;
+    TR_CUDA(c, run_bp(c, BP_WEIGHTS, a, s));
+  }
+  c->w_z0 = z0;
+  c->w_nz = nz;
+  c->w_border = nborder;
+  c->wtvol_ready = true;
   return TR_OK;
+}
+
+// The compact weights of the cached view for a BP_SIRT launch.
+void set_weights(const tr_ctx *c, BpArgs *b) {
+  b->wtvol = c->wtvol_d;
+  b->wslot = c->wslot_d;
+  b->wrow = c->wrow_d;
+  b->wfull = (float)c->nt;
 }
 
 }  // namespace
@@ -614,11 +662,9 @@ tr_status tr_sirt_update(tr_ctx *c, const float *resid, float *vol, int z0, int 
   if (!resid || !vol || z0 < 0 || nz < 1 || z0 + nz > c->th)
     return fail(c, TR_ERR_ARG, "bad SIRT update arguments (z0=%d nz=%d)", z0, nz);
   cudaStream_t s = (cudaStream_t)stream;
-  if ((st = ensure_wtvol(c, s))) return st;
+  if ((st = ensure_wtvol(c, z0, nz, s))) return st;
   BpArgs b = bp_args(c, vol, z0, nz, resid, 0, c->nt, gamma);
-  // The cached weights cover the whole volume; view the same sections.
-  b.wtvol = c->wtvol_d + (c->layout == TR_LAYOUT_Y ? (size_t)z0 * c->nx
-                                                   : (size_t)z0 * c->nx * c->ny);
+  set_weights(c, &b);
   TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   return TR_OK;
 }
@@ -646,14 +692,14 @@ tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gam
   const size_t pn = proj_elems(c);
   if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection"))) return st;
   if ((st = ensure_wt(c, s))) return st;
-  if ((st = ensure_wtvol(c, s))) return st;
+  if ((st = ensure_wtvol(c, 0, c->th, s))) return st;
   for (int it = 0; it < iters; ++it) {
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
     FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
     TR_CUDA(c, launch_fp(c->sep, f, s));
     TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
     BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, 0, c->nt, gamma);
-    b.wtvol = c->wtvol_d;
+    set_weights(c, &b);
     TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
   return TR_OK;
@@ -736,7 +782,7 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
                            "per-tilt maxima"))))
     return st;
   if ((st = ensure_wt(c, s))) return st;
-  if ((st = ensure_wtvol(c, s))) return st;
+  if ((st = ensure_wtvol(c, 0, c->th, s))) return st;
   const float *ps = pdtype == TR_DTYPE_F32 ? nullptr : scale;
   void *res = rdtype == TR_DTYPE_F32 ? (void *)c->val_d : c->res16_d;
   const float *rs = rdtype == TR_DTYPE_F16 ? c->rscale_d : nullptr;
@@ -759,7 +805,7 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
     BpArgs b = bp_args(c, vol, 0, c->th, (const float *)res, 0, c->nt, gamma);
     b.img.dtype = rdtype;
     b.img.scale = rs;
-    b.wtvol = c->wtvol_d;
+    set_weights(c, &b);
     TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
   return TR_OK;

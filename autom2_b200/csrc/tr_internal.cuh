@@ -18,6 +18,7 @@ constexpr int kZG = kThreads / (kTX * kTY);  // 2
 constexpr int kNV = 16;                       // voxels per thread along z
 constexpr int kTZ = kZG * kNV;                // 32
 constexpr int kMaxChunk = 32;                 // tilts staged per chunk (max)
+constexpr int kTileVox = kTX * kTY * kTZ;     // voxels of a back-projection tile
 
 // Forward-projection tile: each lane owns a pair of neighbouring x voxels, so
 // a warp covers 64 x; rows and z groups as above.
@@ -77,6 +78,16 @@ struct BpArgs {
   float gamma;
   const float *wtvol;  // BP_SIRT: per-voxel weight sums (same view strides)
   float *out;          // BP_WEIGHTS: output (same view strides)
+  // Compact voxel weights (wslot != nullptr): tile (bz gy + by) gx + bx of
+  // the view is interior when wslot[tile] < 0 -- every voxel has all four
+  // bilinear neighbours inside the image for every tilt -- and its weight is
+  // wfull (the tilt count; general geometry) or wrow[y] (separable: the
+  // per-row sum of the in-image row weights); a border tile's kTileVox
+  // weights live at wtvol / out + wslot[tile] * kTileVox, voxel
+  // ((wz kNV + k) kTY + wy) kTX + lane.  The weight pass skips interior tiles.
+  const int *wslot;
+  const float *wrow;
+  float wfull;
   int *err;            // err[0]: launch-wide abort word (zero at launch);
                        // err[1]: sticky report word; both set to 1 when a
                        // bounded device wait runs out.  nullptr: no TMA path.
@@ -207,6 +218,14 @@ struct BatchTable {
 // (tr_kernels.cu, tr_filter.cu)
 
 cudaError_t launch_bp(int mode, bool sep, const BpArgs &a, cudaStream_t s);
+// Compact voxel weights: classifies the tiles of view v (slot[tile] = -1
+// interior, else a border slot from *count, which must start at 0), and the
+// separable per-row weights wrow[0..ny) (rows of voxel view v.ny).
+cudaError_t launch_classify_tiles(const TiltGeo *geo, int nt, const VolView &v, float ox, float oy,
+                                  float oz, int pnx, int pny, bool sep, int *slot, int *count,
+                                  cudaStream_t s);
+cudaError_t launch_sep_row_weights(const TiltGeo *geo, int nt, int ny, float oy, int pny,
+                                   float *wrow, cudaStream_t s);
 cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
 cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n, int nsm,
                          cudaStream_t s);

@@ -296,25 +296,44 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
   }
 }
 
-// Epilogue: one coalesced read-modify-write per voxel.
-template <int MODE>
+// Tile index of tile (bx, by, bz) in the compact weights' slot table.
+__device__ __forceinline__ int bp_tile_index(const VolView &v, int bx, int by, int bz) {
+  const int gx = (v.nx + kTX - 1) / kTX, gy = (v.ny + kTY - 1) / kTY;
+  return (bz * gy + by) * gx + bx;
+}
+
+// Epilogue: one coalesced read-modify-write per voxel.  slot: the tile's
+// compact-weight slot (see BpArgs::wslot), -1 interior; unused without them.
+template <int MODE, bool SEP>
 __device__ __forceinline__ void bp_epilogue(const BpArgs &a, const float (&acc)[kNV],
-                                            int x, int y, int zbase) {
+                                            int x, int y, int zbase, int slot) {
   if (x >= a.v.nx || y >= a.v.ny) return;
+  // Voxel k of this thread in a tile's compact weights.
+  const int local0 = (((threadIdx.x >> 5) / kTY) * kNV * kTY + (threadIdx.x >> 5) % kTY) * kTX +
+                     (threadIdx.x & 31);
 #pragma unroll
   for (int k = 0; k < kNV; ++k) {
     const int z = zbase + k;
     if (z >= a.v.nz) break;
     const size_t idx = (size_t)y * a.v.sy + (size_t)z * a.v.sz + x;
+    const size_t cidx = (size_t)slot * kTileVox + local0 + k * (kTY * kTX);
     if (MODE == BP_NORM || MODE == BP_SUM) {
       a.v.vol[idx] += a.gamma * acc[k];
     } else if (MODE == BP_SIRT) {
-      const float w = a.wtvol[idx];
+      float w;
+      if (!a.wslot) w = a.wtvol[idx];
+      else if (slot < 0) w = SEP ? a.wrow[y] : a.wfull;
+      else w = a.wtvol[cidx];
       if (w != 0.f) a.v.vol[idx] += acc[k] / w * a.gamma;
     } else {
-      a.out[idx] = acc[k];
+      a.out[a.wslot ? cidx : idx] = acc[k];
     }
   }
+}
+
+// Slot of tile (bx, by, bz) in the compact weights, or -1.
+__device__ __forceinline__ int bp_tile_slot(const BpArgs &a, int bx, int by, int bz) {
+  return a.wslot ? __ldg(a.wslot + bp_tile_index(a.v, bx, by, bz)) : -1;
 }
 
 // Back-projection with tables staged by the threads from global memory (any
@@ -337,6 +356,9 @@ __global__ void __launch_bounds__(kThreads)
   const int zc = zl + a.v.zoff;
   const int fw = a.fw, fh = SEP ? kTY : a.fh;
   const int pnx = a.img.nx, pny = a.img.ny;
+  const int slot = bp_tile_slot(a, blockIdx.x, blockIdx.y, blockIdx.z);
+  // Compact weights: interior tiles need no weight pass (uniform per CTA).
+  if (MODE == BP_WEIGHTS && a.wslot && slot < 0) return;
 
   float acc[kNV], cmp[kNV];
 #pragma unroll
@@ -384,7 +406,7 @@ __global__ void __launch_bounds__(kThreads)
     bp_accumulate<MODE, SEP, KAHAN>(acc, cmp, tbl_raw, ws, nc, per, fw, pny, lane, wy, wz);
     __syncthreads();
   }
-  bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
+  bp_epilogue<MODE, SEP>(a, acc, xc + lane, yc + wy, zl + wz * kNV, slot);
 }
 
 // ------------------------------------------------------------- TMA staging
@@ -679,7 +701,7 @@ __device__ __forceinline__ bool bp_tma_tile(const BpArgs &a, const CUtensorMap *
   }
   uses[0] += (unsigned)(nchunks + 1) / 2;
   uses[1] += (unsigned)nchunks / 2;
-  bp_epilogue<MODE>(a, acc, xc + lane, yc + wy, zl + wz * kNV);
+  bp_epilogue<MODE, SEP>(a, acc, xc + lane, yc + wy, zl + wz * kNV, bp_tile_slot(a, bx, by, bz));
   return true;
 }
 
@@ -1239,6 +1261,88 @@ __global__ void __launch_bounds__(kThreads, 4) bp_batch_kernel(BatchTable *T) {
                   : bp_tma_tile<BP_SIRT, false, RT>(it.a, &it.map, bx, by, bz, dsm, mbar, uses);
     if (!ok) break;
   }
+}
+
+// ------------------------------------------------------ compact voxel weights
+//
+// A back-projection tile is interior when, for every tilt, the detector
+// coordinates its voxels can reach keep all four bilinear neighbours inside
+// the image (lower neighbour in [0, nx-2] x [0, ny-2], with 1e-3 px of margin
+// over the FP64 extremes for the fixed-point coordinates).  Then every
+// voxel's per-tilt weight sum c is exactly 1 in the weight pass (general
+// geometry: the indicator interpolates to 1.0), so its SIRT weight is the
+// tilt count; with separable geometry the weight depends on the voxel row
+// only (the row pair's in-image weights w0 + w1), so it is the float sum over
+// the tilts, in tilt order, of those -- as the weight pass adds them.
+
+__global__ void classify_tiles_kernel(const TiltGeo *__restrict__ geo, int nt, VolView v,
+                                      float ox, float oy, float oz, int pnx, int pny, int sep,
+                                      int *slot, int *count) {
+  const int gx = (v.nx + kTX - 1) / kTX, gy = (v.ny + kTY - 1) / kTY;
+  const int gz = (v.nz + kTZ - 1) / kTZ;
+  const long long ntiles = (long long)gx * gy * gz;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < ntiles;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int bx = (int)(t % gx), by = (int)((t / gx) % gy), bz = (int)(t / ((long long)gx * gy));
+    const int xc = bx * kTX, yc = by * kTY, zc = bz * kTZ + v.zoff;
+    const double X = (double)((float)xc - ox), Y = (double)((float)yc - oy),
+                 Z = (double)((float)zc - oz);
+    const double ex = kTX - 1, ey = kTY - 1, ez = kTZ - 1, m = 1e-3;
+    bool interior = true;
+    for (int i = 0; i < nt && interior; ++i) {
+      const TiltGeo &g = geo[i];
+      const double uc = g.a[0] + g.a[1] * X + g.a[2] * Y + g.a[3] * Z + (double)ox;
+      const double umin = uc + fmin(0.0, g.a[1] * ex) + fmin(0.0, g.a[2] * ey) +
+                          fmin(0.0, g.a[3] * ez);
+      const double umax = uc + fmax(0.0, g.a[1] * ex) + fmax(0.0, g.a[2] * ey) +
+                          fmax(0.0, g.a[3] * ez);
+      interior = floor(umin - m) >= 0.0 && floor(umax + m) <= pnx - 2;
+      if (!sep) {
+        const double vc = g.b[0] + g.b[1] * X + g.b[2] * Y + g.b[3] * Z + (double)oy;
+        const double vmin = vc + fmin(0.0, g.b[1] * ex) + fmin(0.0, g.b[2] * ey) +
+                            fmin(0.0, g.b[3] * ez);
+        const double vmax = vc + fmax(0.0, g.b[1] * ex) + fmax(0.0, g.b[2] * ey) +
+                            fmax(0.0, g.b[3] * ez);
+        interior = interior && floor(vmin - m) >= 0.0 && floor(vmax + m) <= pny - 2;
+      }
+    }
+    slot[t] = interior ? -1 : atomicAdd(count, 1);
+  }
+}
+
+// Separable per-row weights: wrow[y] = sum over tilts (in order, float) of
+// w0 + w1 for voxel row y, with the rows and weights tile_setup forms.
+__global__ void sep_row_weights_kernel(const TiltGeo *__restrict__ geo, int nt, int ny, float oy,
+                                       int pny, float *wrow) {
+  const int y = blockIdx.x * blockDim.x + threadIdx.x;
+  if (y >= ny) return;
+  float acc = 0.f;
+  for (int i = 0; i < nt; ++i) {
+    const TiltGeo &g = geo[i];
+    const double Yr = (double)((float)y - oy);
+    // b1 = b3 = 0 for separable geometry: v = b0 + b2 Yr + oy (tile_setup).
+    const double vv = g.b[0] + g.b[2] * Yr + (double)oy;
+    const int y0 = (int)floor(vv);
+    const float dy = (float)(vv - (double)y0);
+    const float w0 = (y0 >= 0 && y0 < pny) ? (1 - dy) : 0.f;
+    const float w1 = (y0 + 1 >= 0 && y0 + 1 < pny) ? dy : 0.f;
+    acc += w0 + w1;
+  }
+  wrow[y] = acc;
+}
+
+cudaError_t launch_classify_tiles(const TiltGeo *geo, int nt, const VolView &v, float ox, float oy,
+                                  float oz, int pnx, int pny, bool sep, int *slot, int *count,
+                                  cudaStream_t s) {
+  classify_tiles_kernel<<<1184, 128, 0, s>>>(geo, nt, v, ox, oy, oz, pnx, pny, sep ? 1 : 0, slot,
+                                              count);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sep_row_weights(const TiltGeo *geo, int nt, int ny, float oy, int pny,
+                                   float *wrow, cudaStream_t s) {
+  sep_row_weights_kernel<<<(ny + 127) / 128, 128, 0, s>>>(geo, nt, ny, oy, pny, wrow);
+  return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- launchers

@@ -174,7 +174,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   f.chunk = sg.chunk_fp;
   f.nbound = sg.nbound;
 
-  BpArgs bp;
+  BpArgs bp{};
   bp.v = v;
   bp.img.nx = nx;
   bp.img.ny = ny;
