@@ -141,6 +141,11 @@ def test_cfg1_sirt_converges(engine):
         res.append(float(torch.linalg.vector_norm(
             torch.where(wt != 0, proj - val / torch.where(wt != 0, wt, 1), 0))))
     assert res[0] > res[1] > res[2]
+    # SIRT's voxel weights are compact: interior tiles store none, so the
+    # context's scratch is the two projection-sized buffers plus a small
+    # fraction of a volume (it held a whole volume of weights before).
+    proj_b, vol_b = nt * ny * nx * 4, nx * ny * th * 4
+    assert engine.scratch_bytes < 2 * proj_b + vol_b // 4, engine.scratch_bytes
 
 
 def test_cfg1_half_size_sirt30_whole_volume(engine, reference):
