@@ -82,6 +82,11 @@ struct tr_ctx {
   size_t stage_n = 0;
   cudaEvent_t stage_ev[2] = {nullptr, nullptr};
   int *err_d = nullptr;  // [0] abort word of the current launch, [1] sticky report
+  // z-slab SIRT: the next iteration's reprojection, the device staging slabs
+  // of a host-resident volume, their copy streams and events
+  float *val2_d = nullptr, *slab_d = nullptr;
+  cudaStream_t cp_in = nullptr, cp_out = nullptr;
+  cudaEvent_t ev_in[3] = {}, ev_comp[3] = {}, ev_free[3] = {}, ev_start = nullptr;
 };
 
 namespace {
@@ -273,10 +278,11 @@ tr_status build_filter(tr_ctx *c, int nx) {
   scratch_free(c, (void **)&c->tw_d);
   tr_status s = scratch_alloc(c, (void **)&c->ghat_d, sizeof(float2) * M, "filter spectrum");
   if (s) return s;
-  s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * M, "filter twiddles");
+  s = scratch_alloc(c, (void **)&c->tw_d, sizeof(float2) * sp.tw.size(), "filter twiddles");
   if (s) return s;
   TR_CUDA(c, cudaMemcpy(c->ghat_d, sp.ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-  TR_CUDA(c, cudaMemcpy(c->tw_d, sp.tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+  TR_CUDA(c, cudaMemcpy(c->tw_d, sp.tw.data(), sizeof(float2) * sp.tw.size(),
+                        cudaMemcpyHostToDevice));
   c->filt_nx = nx;
   c->filt_npad = sp.npad;
   c->filt_log2m = sp.log2m;
@@ -420,6 +426,205 @@ void set_weights(const tr_ctx *c, BpArgs *b) {
   b->wfull = (float)c->nt;
 }
 
+// ---------------------------------------------------------------- z-slabs
+// SIRT over slabs of `depth` sections (TiltRecZ's split of the volume along
+// z, main-mpiz.cpp:1054-1069, with CuSIRTZ's iteration, recon_z.cu:85-190).
+// Each iteration is one sweep over the slabs: back-project the residual into
+// slab k with the update, then forward-project the updated slab into the next
+// iteration's reprojection sums.  A host-resident volume is staged slab by
+// slab through three device buffers: the copy in of slab k+1 and the copy out
+// of slab k-1 run on their own streams while slab k computes.
+constexpr int kSlabBufs = 3;
+
+struct SlabRun {
+  const void *proj;
+  int pdtype;
+  const float *pscale;
+  int rdtype;
+  float *vol;
+  bool host;
+  int iters;
+  float gamma;
+  int depth;
+};
+
+// Slab depth used for `want` sections: the whole thickness, or a multiple of
+// the tile depth (the slab boundaries are tile boundaries, so each slab's
+// tiles are the whole volume's and share its compact voxel weights).
+int slab_depth(const tr_ctx *c, int want) {
+  if (want >= c->th) return c->th;
+  return std::max(kTZ, want / kTZ * kTZ);
+}
+
+size_t slab_elems(const tr_ctx *c, int depth) { return (size_t)c->nx * c->ny * depth; }
+
+// Volume view of sections [z0, z0 + nz): the caller's device volume, or a
+// staging buffer holding just those sections ([ny][nz][nx] in the Y layout).
+VolView slab_view(const tr_ctx *c, float *base, bool staged, int z0, int nz) {
+  if (!staged) {
+    const size_t off = c->layout == TR_LAYOUT_Y ? (size_t)z0 * c->nx
+                                                : (size_t)z0 * c->nx * c->ny;
+    return full_view(c, base + off, z0, nz);
+  }
+  VolView v = full_view(c, base, z0, nz);
+  if (c->layout == TR_LAYOUT_Y) v.sy = (long long)nz * c->nx;
+  return v;
+}
+
+cudaError_t slab_copy(const tr_ctx *c, float *dev, float *host, int z0, int nz, bool to_dev,
+                      cudaStream_t s) {
+  const size_t nx = c->nx, ny = c->ny;
+  const cudaMemcpyKind k = to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+  if (c->layout == TR_LAYOUT_Z) {
+    float *h = host + (size_t)z0 * nx * ny;
+    return to_dev ? cudaMemcpyAsync(dev, h, nx * ny * nz * sizeof(float), k, s)
+                  : cudaMemcpyAsync(h, dev, nx * ny * nz * sizeof(float), k, s);
+  }
+  // Y layout: ny runs of nz rows, one strided copy.
+  float *h = host + (size_t)z0 * nx;
+  const size_t w = nx * nz * sizeof(float), hp = nx * (size_t)c->th * sizeof(float);
+  return to_dev ? cudaMemcpy2DAsync(dev, w, h, hp, w, ny, k, s)
+                : cudaMemcpy2DAsync(h, hp, dev, w, w, ny, k, s);
+}
+
+tr_status slab_streams(tr_ctx *c) {
+  if (c->cp_in) return TR_OK;
+  TR_CUDA(c, cudaStreamCreateWithFlags(&c->cp_in, cudaStreamNonBlocking));
+  TR_CUDA(c, cudaStreamCreateWithFlags(&c->cp_out, cudaStreamNonBlocking));
+  for (int i = 0; i < kSlabBufs; ++i) {
+    TR_CUDA(c, cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming));
+    TR_CUDA(c, cudaEventCreateWithFlags(&c->ev_comp[i], cudaEventDisableTiming));
+    TR_CUDA(c, cudaEventCreateWithFlags(&c->ev_free[i], cudaEventDisableTiming));
+  }
+  TR_CUDA(c, cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming));
+  return TR_OK;
+}
+
+// Scratch of the slab path: both reprojections, the 16-bit residual, the
+// weights of the whole volume, and the staging slabs of a host volume.
+tr_status slab_scratch(tr_ctx *c, const SlabRun &r, cudaStream_t s) {
+  const size_t pn = proj_elems(c);
+  tr_status st;
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection")) ||
+      (st = scratch_alloc(c, (void **)&c->val2_d, pn * sizeof(float), "next reprojection")))
+    return st;
+  if (r.rdtype != TR_DTYPE_F32 &&
+      (st = scratch_alloc(c, &c->res16_d, pn * 2, "16-bit residual")))
+    return st;
+  if (r.rdtype == TR_DTYPE_F16 &&
+      ((st = scratch_alloc(c, (void **)&c->rscale_d, sizeof(float) * c->nt,
+                           "residual scales")) ||
+       (st = scratch_alloc(c, (void **)&c->maxbits_d, sizeof(unsigned) * c->nt,
+                           "per-tilt maxima"))))
+    return st;
+  if (r.host &&
+      (st = scratch_alloc(c, (void **)&c->slab_d,
+                          kSlabBufs * slab_elems(c, r.depth) * sizeof(float), "z-slab staging")))
+    return st;
+  if ((st = ensure_wt(c, s))) return st;
+  if ((st = ensure_wtvol(c, 0, c->th, s))) return st;
+  return slab_streams(c);
+}
+
+// Residual of the reprojection `val` (in place) and its 16-bit copy; returns
+// the image the back-projection reads.
+tr_status slab_residual(tr_ctx *c, const SlabRun &r, float *val, cudaStream_t s,
+                        const void **res, const float **rs) {
+  const size_t plane = (size_t)c->nx * c->ny;
+  const float *ps = r.pdtype == TR_DTYPE_F32 ? nullptr : r.pscale;
+  if (r.rdtype == TR_DTYPE_F16) {
+    TR_CUDA(c, launch_resid_lp(r.proj, r.pdtype, ps, val, c->wt_d, plane, c->nt, TR_DTYPE_F32,
+                               val, nullptr, c->nsm, s));
+    TR_CUDA(c, launch_quantize(val, plane, c->nt, TR_DTYPE_F16, c->res16_d, c->rscale_d,
+                               c->maxbits_d, c->nsm, s));
+    *res = c->res16_d;
+    *rs = c->rscale_d;
+  } else {
+    void *out = r.rdtype == TR_DTYPE_F32 ? (void *)val : c->res16_d;
+    TR_CUDA(c, launch_resid_lp(r.proj, r.pdtype, ps, val, c->wt_d, plane, c->nt, r.rdtype, out,
+                               nullptr, c->nsm, s));
+    *res = out;
+    *rs = nullptr;
+  }
+  return TR_OK;
+}
+
+// One sweep over the slabs of sections [0, zend): with `res`, the SIRT
+// update of each slab from that residual; with `fp_out`, the forward
+// projection of each (updated) slab added into fp_out.  A host volume is
+// copied in before and, after an update, out again.
+tr_status slab_sweep(tr_ctx *c, const SlabRun &r, int zend, const void *res, const float *rs,
+                     float *fp_out, cudaStream_t s) {
+  const dim3 g = bp_tile_grid(full_view(c, nullptr, 0, c->th));
+  const bool write_back = res != nullptr;
+  if (r.host) {
+    TR_CUDA(c, cudaEventRecord(c->ev_start, s));
+    TR_CUDA(c, cudaStreamWaitEvent(c->cp_in, c->ev_start, 0));
+  }
+  int k = 0, used = 0;
+  for (int z0 = 0; z0 < zend; z0 += r.depth, k = (k + 1) % kSlabBufs, ++used) {
+    const int nz = std::min(r.depth, zend - z0);
+    float *buf = r.host ? c->slab_d + k * slab_elems(c, r.depth) : r.vol;
+    if (r.host) {
+      if (used >= kSlabBufs) TR_CUDA(c, cudaStreamWaitEvent(c->cp_in, c->ev_free[k], 0));
+      TR_CUDA(c, slab_copy(c, buf, r.vol, z0, nz, true, c->cp_in));
+      TR_CUDA(c, cudaEventRecord(c->ev_in[k], c->cp_in));
+      TR_CUDA(c, cudaStreamWaitEvent(s, c->ev_in[k], 0));
+    }
+    const VolView v = slab_view(c, buf, r.host, z0, nz);
+    if (res) {
+      BpArgs b = bp_args(c, nullptr, z0, nz, (const float *)res, 0, c->nt, r.gamma);
+      b.v = v;
+      b.img.dtype = r.rdtype;
+      b.img.scale = rs;
+      set_weights(c, &b);
+      b.wslot = c->wslot_d + (size_t)(z0 / kTZ) * g.x * g.y;  // this slab's tiles
+      TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
+    }
+    if (fp_out) {
+      FpArgs f = fp_args(c, nullptr, z0, nz, fp_out, 0, c->nt);
+      f.v = v;
+      TR_CUDA(c, launch_fp(c->sep, f, s));
+    }
+    if (r.host) {
+      if (write_back) {
+        TR_CUDA(c, cudaEventRecord(c->ev_comp[k], s));
+        TR_CUDA(c, cudaStreamWaitEvent(c->cp_out, c->ev_comp[k], 0));
+        TR_CUDA(c, slab_copy(c, buf, r.vol, z0, nz, false, c->cp_out));
+        TR_CUDA(c, cudaEventRecord(c->ev_free[k], c->cp_out));
+      } else {
+        TR_CUDA(c, cudaEventRecord(c->ev_free[k], s));
+      }
+    }
+  }
+  if (r.host && write_back) {  // the volume is complete when `s` reaches here
+    TR_CUDA(c, cudaEventRecord(c->ev_start, c->cp_out));
+    TR_CUDA(c, cudaStreamWaitEvent(s, c->ev_start, 0));
+  }
+  return TR_OK;
+}
+
+tr_status slab_sirt(tr_ctx *c, const SlabRun &r, cudaStream_t s) {
+  tr_status st = slab_scratch(c, r, s);
+  if (st) return st;
+  const size_t pn = proj_elems(c);
+  float *cur = c->val_d, *next = c->val2_d;
+  if (r.iters == 0) return TR_OK;
+  TR_CUDA(c, cudaMemsetAsync(cur, 0, pn * sizeof(float), s));
+  if ((st = slab_sweep(c, r, c->th, nullptr, nullptr, cur, s))) return st;
+  for (int it = 0; it < r.iters; ++it) {
+    const void *res;
+    const float *rs;
+    if ((st = slab_residual(c, r, cur, s, &res, &rs))) return st;
+    const bool more = it + 1 < r.iters;
+    if (more) TR_CUDA(c, cudaMemsetAsync(next, 0, pn * sizeof(float), s));
+    if ((st = slab_sweep(c, r, c->th, res, rs, more ? next : nullptr, s))) return st;
+    std::swap(cur, next);
+  }
+  if (r.host) TR_CUDA(c, cudaStreamSynchronize(s));
+  return TR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -514,6 +719,12 @@ tr_status tr_destroy(tr_ctx *c) {
     if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
   }
   if (c->io_stream) cudaStreamDestroy(c->io_stream);
+  if (c->cp_in) cudaStreamDestroy(c->cp_in);
+  if (c->cp_out) cudaStreamDestroy(c->cp_out);
+  for (int i = 0; i < 3; ++i)
+    for (cudaEvent_t e : {c->ev_in[i], c->ev_comp[i], c->ev_free[i]})
+      if (e) cudaEventDestroy(e);
+  if (c->ev_start) cudaEventDestroy(c->ev_start);
   if (c->err_d) cudaFree(c->err_d);
   delete c;
   return TR_OK;
@@ -808,6 +1019,87 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
     set_weights(c, &b);
     TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
+  return TR_OK;
+}
+
+tr_status tr_sirt_zslabs(tr_ctx *c, const void *proj, int pdtype, const float *scale,
+                         int rdtype, float *vol, int vol_on_host, int iters, float gamma,
+                         int depth, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  auto ok_dtype = [](int d) {
+    return d == TR_DTYPE_F32 || d == TR_DTYPE_F16 || d == TR_DTYPE_BF16;
+  };
+  if (!proj || !vol || iters < 0 || depth < 1 || !ok_dtype(pdtype) || !ok_dtype(rdtype) ||
+      (pdtype != TR_DTYPE_F32 && !scale))
+    return fail(c, TR_ERR_ARG, "bad z-slab SIRT arguments (depth %d, dtypes %d/%d)", depth,
+                pdtype, rdtype);
+  SlabRun r{proj, pdtype, scale, rdtype, vol, vol_on_host != 0, iters, gamma,
+            slab_depth(c, depth)};
+  st = slab_sirt(c, r, (cudaStream_t)stream);
+  if (!st && r.host) st = take_timeout(c);
+  return st;
+}
+
+tr_status tr_autotune_zslab(tr_ctx *c, const void *proj, int pdtype, const float *scale,
+                            int rdtype, float *vol, int vol_on_host, int *depth_out,
+                            double *sweep_ms) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || !depth_out || (pdtype != TR_DTYPE_F32 && !scale))
+    return fail(c, TR_ERR_ARG, "bad z-slab autotune arguments");
+  cudaStream_t s = c->io_stream;
+  cudaEvent_t e0, e1;
+  TR_CUDA(c, cudaEventCreate(&e0));
+  TR_CUDA(c, cudaEventCreate(&e1));
+  int best = 0;
+  double best_ms = 0;
+  int last = 0;
+  for (int want : {32, 64, 128, 256, 512}) {
+    const int d = slab_depth(c, want);
+    if (d == last) continue;
+    last = d;
+    // gamma 0 over a zero residual: the sweep does the full work (copies,
+    // update, forward projection) and leaves the volume's values unchanged.
+    SlabRun r{proj, pdtype, scale, rdtype, vol, vol_on_host != 0, 1, 0.f, d};
+    if ((st = slab_scratch(c, r, s))) {
+      if (st == TR_ERR_BUDGET || st == TR_ERR_OOM) continue;  // this depth does not fit
+      break;
+    }
+    const size_t pn = proj_elems(c);
+    const void *res = rdtype == TR_DTYPE_F32 ? (const void *)c->val_d : c->res16_d;
+    const float *rs = rdtype == TR_DTYPE_F16 ? c->rscale_d : nullptr;
+    cudaError_t e = cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s);
+    if (e == cudaSuccess && rdtype != TR_DTYPE_F32) e = cudaMemsetAsync(c->res16_d, 0, pn * 2, s);
+    if (e == cudaSuccess && rs) e = cudaMemsetAsync(c->rscale_d, 0, c->nt * sizeof(float), s);
+    if (e != cudaSuccess) {
+      st = cuda_fail(c, e, "clearing the autotune residual");
+      break;
+    }
+    double ms = 0;
+    for (int rep = 0; rep < 2 && !st; ++rep) {  // the first sweep warms up
+      st = cudaEventRecord(e0, s) ? TR_ERR_CUDA : TR_OK;
+      if (!st) st = slab_sweep(c, r, c->th, res, rs, c->val2_d, s);
+      if (!st && cudaEventRecord(e1, s)) st = TR_ERR_CUDA;
+      if (!st && cudaEventSynchronize(e1)) st = TR_ERR_CUDA;
+      float f = 0;
+      if (!st) cudaEventElapsedTime(&f, e0, e1);
+      ms = f;
+    }
+    if (st) break;
+    if (!best || ms < best_ms) {
+      best = d;
+      best_ms = ms;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st && st != TR_ERR_BUDGET && st != TR_ERR_OOM) return st;
+  if (!best) return fail(c, TR_ERR_BUDGET, "no slab depth fits the budget");
+  if ((st = take_timeout(c))) return st;
+  c->err.clear();
+  *depth_out = best;
+  if (sweep_ms) *sweep_ms = best_ms;
   return TR_OK;
 }
 

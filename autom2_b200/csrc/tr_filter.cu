@@ -11,19 +11,28 @@
 // nx = 256..4096), so the circular convolution is evaluated as a linear one on
 // a power-of-two length M >= N + nx - 1 with the kernel laid out for
 // lags -(N-1)..nx-1; no wrap-around reaches the kept outputs.  The kernel's
-// spectrum (already scaled by 1/(M nx) and permuted to bit-reversed order) is
-// built once on the host in double precision.
+// spectrum (already scaled by 1/(M nx), natural order) is built once on the
+// host in double precision.
 //
-// Per CTA: rows r and r+1 become the real and imaginary parts of one complex
-// sequence of M points in shared memory; a Stockham autosort FFT (radix-4
-// passes, one radix-2 pass first when log2 M is odd; each thread holds its
-// butterflies' points in registers between a load and a store phase), a
-// pointwise product with the spectrum, and the inverse transform give both
-// filtered rows at once because the kernel is real.
+// Per row pair: rows r and r+1 become the real and imaginary parts of one
+// complex sequence of M points in shared memory, transformed by a Stockham
+// autosort FFT, multiplied by the spectrum and transformed back; both rows
+// come out filtered at once because the kernel is real.  Each thread holds
+// 16 P points in registers per pass (P = 1, or 2 for M = 16384 so that the
+// block stays at 512 threads): radix-16 passes, after one radix-2/4/8 pass
+// when log2 M is not a multiple of 4, so M = 4096 takes 3 passes each way.
+// A pass is a shared-memory load, a barrier, twiddles and 16-point DFTs in
+// registers, and a store.  Shared memory holds one pad entry after every 16
+// points, which spreads the strided stores of the early passes over all
+// banks.  Twiddles come from per-pass tables, [r - 1][k] for the radix-16
+// pass with sub-transform size Ns (e^{-2 pi i r k / (16 Ns)}), read through
+// L1 with consecutive threads on consecutive entries.  CTAs are persistent
+// and loop over row pairs.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
+#include "tr_filter_host.h"
 #include "tr_internal.cuh"
 
 namespace trb {
@@ -34,122 +43,196 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 
-constexpr int kFftMaxB = 4;  // butterflies per thread and pass (launcher sizes the block)
+// Shared-memory slot of point i: one pad entry after every 16 points.
+__device__ __forceinline__ int fft_slot(int i) { return i + (i >> 4); }
 
-// One Stockham pass of radix R over buf[0..M) (M = 2^log2m), sub-transform
-// size Ns = 2^log2ns before the pass: butterfly j reads points j + r M/R,
-// multiplies point r by w^{r (j mod Ns)} with w = e^{DIR 2 pi i / (Ns R)},
-// transforms the R points and writes them to (j / Ns) Ns R + (j mod Ns) +
-// r Ns.  DIR = -1 forward, +1 inverse (unscaled).  tw[t] = e^{-2 pi i t / M}.
-template <int R, int DIR>
-__device__ __forceinline__ void stockham_pass(float2 *buf, int log2m, int log2ns,
-                                              const float2 *__restrict__ tw) {
-  const int M = 1 << log2m, nb = M / R, Ns = 1 << log2ns;
-  constexpr int lr = R == 4 ? 2 : 1;
-  float2 v[kFftMaxB][R];
-#pragma unroll
-  for (int b = 0; b < kFftMaxB; ++b) {
-    const int j = threadIdx.x + b * blockDim.x;
-    if (j < nb) {
-#pragma unroll
-      for (int r = 0; r < R; ++r) v[b][r] = buf[j + r * nb];
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int b = 0; b < kFftMaxB; ++b) {
-    const int j = threadIdx.x + b * blockDim.x;
-    if (j < nb) {
-      const int k = j & (Ns - 1);
-      const int step = k << (log2m - log2ns - lr);  // k M / (Ns R)
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 w = __ldg(tw + ((r * step) & (M - 1)));
-        if (DIR > 0) w.y = -w.y;
-        v[b][r] = cmul(v[b][r], w);
-      }
-      float2 o[R];
-      if (R == 2) {
-        o[0] = cadd(v[b][0], v[b][1]);
-        o[1] = csub(v[b][0], v[b][1]);
-      } else {
-        const float2 y0 = cadd(v[b][0], v[b][2]), y1 = csub(v[b][0], v[b][2]);
-        const float2 y2 = cadd(v[b][1], v[b][3]), d = csub(v[b][1], v[b][3]);
-        // forward: -i d; inverse: +i d
-        const float2 y3 = DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);
-        o[0] = cadd(y0, y2);
-        o[1] = cadd(y1, y3);
-        o[2] = csub(y0, y2);
-        o[3] = csub(y1, y3);
-      }
-      const int base = ((j - k) << lr) + k;
-#pragma unroll
-      for (int r = 0; r < R; ++r) buf[base + r * Ns] = o[r];
-    }
-  }
-  __syncthreads();
+// e^{DIR 2 pi i m / 16} for a compile-time m (after unrolling).
+template <int DIR>
+__device__ __forceinline__ float2 w16(int m) {
+  constexpr float c[16] = {1.f, 0.92387953f, 0.70710678f, 0.38268343f, 0.f, -0.38268343f,
+                           -0.70710678f, -0.92387953f, -1.f, -0.92387953f, -0.70710678f,
+                           -0.38268343f, 0.f, 0.38268343f, 0.70710678f, 0.92387953f};
+  m &= 15;
+  return make_float2(c[m], (float)DIR * c[(m + 12) & 15]);  // sin(x) = cos(x - pi/2)
 }
 
 template <int DIR>
-__device__ __forceinline__ void stockham_fft(float2 *buf, int log2m, const float2 *tw) {
-  int ls = 0;
-  if (log2m & 1) {
-    stockham_pass<2, DIR>(buf, log2m, 0, tw);
-    ls = 1;
-  }
-  for (; ls < log2m; ls += 2) stockham_pass<4, DIR>(buf, log2m, ls, tw);
+__device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3) {
+  const float2 y0 = cadd(a0, a2), y1 = csub(a0, a2), y2 = cadd(a1, a3), d = csub(a1, a3);
+  const float2 y3 = DIR < 0 ? make_float2(d.y, -d.x) : make_float2(-d.y, d.x);  // DIR i d
+  a0 = cadd(y0, y2);
+  a1 = cadd(y1, y3);
+  a2 = csub(y0, y2);
+  a3 = csub(y1, y3);
 }
 
-__global__ void __launch_bounds__(1024) rweight_kernel(const FilterArgs f) {
+// In-place R-point DFT of v[0..R) (R = 2, 4, 8, 16; sign DIR); output X[r]
+// ends at v[dft_pos<R>(r)]: (R/4) (r % 4) + r / 4 for R = 8, 16 and r
+// otherwise (Cooley-Tukey with n = (R/4) n1 + n2, k = k1 + 4 k2).
+template <int R>
+__device__ __forceinline__ constexpr int dft_pos(int r) {
+  return R >= 8 ? (R / 4) * (r % 4) + r / 4 : r;
+}
+template <int R, int DIR>
+__device__ __forceinline__ void dft_r(float2 *v) {
+  if (R == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    dft4<DIR>(v[0], v[1], v[2], v[3]);
+  } else {
+    constexpr int Q = R / 4;  // 2 or 4
+#pragma unroll
+    for (int n2 = 0; n2 < Q; ++n2) dft4<DIR>(v[n2], v[Q + n2], v[2 * Q + n2], v[3 * Q + n2]);
+    // now v[n2 + Q k1] = Y[n2][k1]; twiddle by e^{DIR 2 pi i n2 k1 / R}
+#pragma unroll
+    for (int n2 = 1; n2 < Q; ++n2)
+#pragma unroll
+      for (int k1 = 1; k1 < 4; ++k1) v[n2 + Q * k1] = cmul(v[n2 + Q * k1], w16<DIR>(n2 * k1 * (16 / R)));
+    // DFT over n2 for each k1: X[k1 + 4 k2] = sum_n2 Y[n2][k1] W_Q^{n2 k2}
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      float2 *y = v + Q * k1;
+      if (Q == 2) {
+        const float2 a = y[0], b = y[1];
+        y[0] = cadd(a, b);
+        y[1] = csub(a, b);
+      } else {
+        dft4<DIR>(y[0], y[1], y[2], y[3]);
+      }
+    }
+  }
+}
+
+// One Stockham pass of radix R over the M = 2^log2m points in buf, with
+// sub-transform size Ns = 2^log2ns: butterfly j reads points j + r M/R,
+// multiplies point r by w^{r (j mod Ns)} with w = e^{DIR 2 pi i / (Ns R)},
+// transforms the R points and writes point r to (j / Ns) Ns R + (j mod Ns) +
+// r Ns.  Each thread takes 16 P / R butterflies j = tid + b blockDim.x
+// (blockDim.x = M / (16 P) exactly).  tw: this pass's table, [r - 1][k] for
+// k < Ns (radix 16 only; passes with Ns = 1 have no twiddles).
+template <int R, int DIR, int P>
+__device__ __forceinline__ void stockham_pass(float2 *buf, int log2m, int log2ns,
+                                              const float2 *__restrict__ tw) {
+  constexpr int B = 16 * P / R;
+  constexpr int lr = R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1;
+  const int nb = (1 << log2m) >> lr, Ns = 1 << log2ns;
+  float2 v[16 * P];
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    const int j = threadIdx.x + b * blockDim.x;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[b * R + r] = buf[fft_slot(j + r * nb)];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; ++b) {
+    const int j = threadIdx.x + b * blockDim.x;
+    const int k = j & (Ns - 1);
+    if (R == 16 && log2ns > 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 w = __ldg(tw + (r - 1) * Ns + k);
+        if (DIR > 0) w.y = -w.y;
+        v[b * R + r] = cmul(v[b * R + r], w);
+      }
+    }
+    dft_r<R, DIR>(v + b * R);
+    const int base = ((j - k) << lr) + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[fft_slot(base + r * Ns)] = v[b * R + dft_pos<R>(r)];
+  }
+  __syncthreads();
+}
+
+// R0: radix of the first pass (2, 4 or 8 = 2^(log2m mod 4)), or 16 when
+// log2m is a multiple of 4.  A template parameter rather than a switch: one
+// code path per instantiation keeps the register allocation at one pass's.
+template <int DIR, int P, int R0>
+__device__ __forceinline__ void stockham_fft(float2 *buf, int log2m, const float2 *tw) {
+  int ls = 0;
+  if (R0 < 16) {
+    stockham_pass<R0, DIR, P>(buf, log2m, 0, tw);
+    ls = log2m & 3;
+  }
+  for (; ls < log2m; ls += 4) {
+    stockham_pass<16, DIR, P>(buf, log2m, ls, tw);
+    if (ls > 0) tw += 15 << ls;
+  }
+}
+
+template <int P, int R0>
+__global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
   extern __shared__ float2 buf[];
   const int M = 1 << f.log2m;
-  const long long r0 = 2ll * blockIdx.x;
-  const bool has1 = r0 + 1 < f.nrows;
-  const float *x0 = f.rows + r0 * f.nx;
-  const float *x1 = has1 ? x0 + f.nx : nullptr;
+  const long long npairs = (f.nrows + 1) / 2;
   const int nx = f.nx, N = f.n_pad;
   const int nxp = N - nx + 1;
-  const float a0 = x0[0], b0 = x0[nx - 1];
-  const float a1 = has1 ? x1[0] : 0.f, b1 = has1 ? x1[nx - 1] : 0.f;
-
-  // Padded rows (buf2fft_padding_1D, filter_prj.cpp:652-672), zero beyond N.
-  for (int j = threadIdx.x; j < M; j += blockDim.x) {
-    float re = 0.f, im = 0.f;
-    if (j < nx) {
-      re = x0[j];
-      im = has1 ? x1[j] : 0.f;
-    } else if (j < N) {
-      const float wa = (float)(j - nx + 1) / (float)nxp;
-      const float wb = (float)(N - j) / (float)nxp;
-      re = wa * a0 + wb * b0;
-      im = wa * a1 + wb * b1;
+  for (long long pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
+    const long long r0 = 2 * pair;
+    const bool has1 = r0 + 1 < f.nrows;
+    const float *x0 = f.rows + r0 * f.nx;
+    const float *x1 = has1 ? x0 + f.nx : nullptr;
+    const float a0 = x0[0], b0 = x0[nx - 1];
+    const float a1 = has1 ? x1[0] : 0.f, b1 = has1 ? x1[nx - 1] : 0.f;
+    // Padded rows (buf2fft_padding_1D, filter_prj.cpp:652-672), zero beyond N.
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+      float re = 0.f, im = 0.f;
+      if (j < nx) {
+        re = x0[j];
+        im = has1 ? x1[j] : 0.f;
+      } else if (j < N) {
+        const float wa = (float)(j - nx + 1) / (float)nxp;
+        const float wb = (float)(N - j) / (float)nxp;
+        re = wa * a0 + wb * b0;
+        im = wa * a1 + wb * b1;
+      }
+      buf[fft_slot(j)] = make_float2(re, im);
     }
-    buf[j] = make_float2(re, im);
+    __syncthreads();
+    stockham_fft<-1, P, R0>(buf, f.log2m, f.tw);
+    for (int j = threadIdx.x; j < M; j += blockDim.x)
+      buf[fft_slot(j)] = cmul(buf[fft_slot(j)], __ldg(f.ghat + j));
+    __syncthreads();
+    stockham_fft<1, P, R0>(buf, f.log2m, f.tw);
+    float *y0 = f.rows + r0 * f.nx;
+    for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+      const float2 z = buf[fft_slot(j)];
+      y0[j] = z.x;
+      if (has1) y0[f.nx + j] = z.y;
+    }
+    __syncthreads();  // buf is reused by the next pair
   }
-  __syncthreads();
-  stockham_fft<-1>(buf, f.log2m, f.tw);
-  for (int j = threadIdx.x; j < M; j += blockDim.x) buf[j] = cmul(buf[j], __ldg(f.ghat + j));
-  __syncthreads();
-  stockham_fft<1>(buf, f.log2m, f.tw);
-  float *y0 = f.rows + r0 * f.nx;
-  for (int j = threadIdx.x; j < nx; j += blockDim.x) {
-    const float2 z = buf[j];
-    y0[j] = z.x;
-    if (has1) y0[f.nx + j] = z.y;
-  }
+}
+
+template <int P, int R0>
+static cudaError_t launch_rweight_p(const FilterArgs &f, cudaStream_t s) {
+  const int M = 1 << f.log2m;
+  const size_t smem = (size_t)(M + M / 16) * sizeof(float2);
+  cudaError_t e = cudaFuncSetAttribute(
+      rweight_kernel<P, R0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const long long pairs = (f.nrows + 1) / 2;
+  const int threads = M / (16 * P);
+  int dev = 0, nsm = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rweight_kernel<P, R0>, threads, smem);
+  const long long grid = std::min<long long>(pairs, (long long)nsm * std::max(1, per_sm));
+  rweight_kernel<P, R0><<<(unsigned)std::max<long long>(1, grid), threads, smem, s>>>(f);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_rweight(const FilterArgs &f, cudaStream_t s) {
-  const int M = 1 << f.log2m;
-  const size_t smem = (size_t)M * sizeof(float2);
-  cudaError_t e = cudaFuncSetAttribute(
-      rweight_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  const long long pairs = (f.nrows + 1) / 2;
-  // At most kFftMaxB butterflies per thread in a radix-2 pass (M/2 of them).
-  const int threads = std::min(1024, std::max(64, M / (2 * kFftMaxB)));
-  rweight_kernel<<<(unsigned)pairs, threads, smem, s>>>(f);
-  return cudaGetLastError();
+  if (f.log2m < kRweightMinLog2 || f.log2m > kRweightMaxLog2) return cudaErrorInvalidValue;
+  if (f.log2m == 14) return launch_rweight_p<2, 4>(f, s);
+  switch (f.log2m & 3) {
+    case 1: return launch_rweight_p<1, 2>(f, s);
+    case 2: return launch_rweight_p<1, 4>(f, s);
+    case 3: return launch_rweight_p<1, 8>(f, s);
+    default: return launch_rweight_p<1, 16>(f, s);
+  }
 }
 
 // ------------------------------------------------------------- FBP filters

@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -33,22 +34,31 @@ inline void fft_host(std::vector<std::complex<double>> &x) {
   }
 }
 
+// FFT sizes the device filter handles: M = 2^4 .. 2^14 (nx up to about 7800).
+constexpr int kRweightMinLog2 = 4;
+constexpr int kRweightMaxLog2 = 14;
+
 struct RweightSpectrum {
   int npad = 0;   // padded row length nx + nx/10 of the reference
   int log2m = 0;  // FFT size 2^log2m >= npad + nx - 1
   std::vector<float2> ghat;  // kernel spectrum, natural order, scaled 1/(M nx)
-  std::vector<float2> tw;    // twiddles e^{-2 pi i k / M}, k < M
+  // Twiddles of the radix-16 Stockham passes with sub-transform size
+  // Ns = 2^ls > 1 (ls = log2m mod 4, then every 4th value below log2m), one
+  // table per pass in that order: entry [r - 1][k] = e^{-2 pi i r k / (16 Ns)}
+  // for r = 1..15, k < Ns.
+  std::vector<float2> tw;
 };
 
-// False when the FFT would not fit `smem_max` bytes of complex floats.
+// False when the FFT (M points plus one pad entry per 16) would not fit
+// `smem_max` bytes of shared memory.
 inline bool rweight_spectrum(int nx, size_t smem_max, RweightSpectrum *out) {
   const int N = nx + nx / 10;
-  int log2m = 1;
+  int log2m = kRweightMinLog2;
   while ((1 << log2m) < N + nx - 1) ++log2m;
   const int M = 1 << log2m;
   out->npad = N;
   out->log2m = log2m;
-  if ((size_t)M * sizeof(float2) > smem_max || log2m > 14) return false;
+  if ((size_t)(M + M / 16) * sizeof(float2) > smem_max || log2m > kRweightMaxLog2) return false;
   // Weights exactly as filter_prj.cpp:694-723 forms them (float arithmetic).
   const int r = (int)floor((float)N * 0.05f);
   const float sg = (float)N * 0.5f;
@@ -76,12 +86,20 @@ inline bool rweight_spectrum(int nx, size_t smem_max, RweightSpectrum *out) {
   for (int e = -(N - 1); e <= nx - 1; ++e) g[(e % M + M) % M] = h[(e % N + N) % N];
   fft_host(g);
   out->ghat.resize(M);
-  out->tw.resize(M);
   const double scale = 1.0 / ((double)M * nx);
   for (int i = 0; i < M; ++i)
     out->ghat[i] = make_float2((float)(g[i].real() * scale), (float)(g[i].imag() * scale));
-  for (int k = 0; k < M; ++k)
-    out->tw[k] = make_float2((float)cos(2.0 * M_PI * k / M), (float)-sin(2.0 * M_PI * k / M));
+  out->tw.clear();
+  for (int ls = log2m & 3; ls < log2m; ls += 4) {
+    if (ls == 0) continue;
+    const int ns = 1 << ls;
+    for (int r = 1; r < 16; ++r)
+      for (int k = 0; k < ns; ++k) {
+        const double a = -2.0 * M_PI * r * k / (16.0 * ns);
+        out->tw.push_back(make_float2((float)cos(a), (float)sin(a)));
+      }
+  }
+  if (out->tw.empty()) out->tw.push_back(make_float2(1.f, 0.f));  // keep the buffer non-empty
   return true;
 }
 

@@ -150,7 +150,7 @@ struct FilterArgs {
   int nx, n_pad;        // row length and the reference's padded length N
   int log2m;            // M = 1 << log2m
   const float2 *ghat;   // [M] kernel spectrum, natural order, scaled
-  const float2 *tw;     // [M] e^{-2 pi i k / M}
+  const float2 *tw;     // two-level twiddles (tr_filter_host.h RweightSpectrum::tw)
 };
 
 // ------------------------------------------------------------ batched steps

@@ -65,6 +65,8 @@ struct Job {
   // device memory owned by the job (stream-ordered allocations)
   TiltGeo *geo = nullptr;
   float *val = nullptr, *wt = nullptr, *wtvol = nullptr, *vol_own = nullptr;
+  float *wrow = nullptr;  // separable per-row voxel weights
+  int *wslot = nullptr;   // compact voxel weights: a slot per tile, then the border count
   void *pstore = nullptr, *res = nullptr;
   float *pscale = nullptr, *rscale = nullptr;
   unsigned *maxbits = nullptr;
@@ -75,6 +77,8 @@ struct Job {
   const float *ps = nullptr, *rs = nullptr;
   BatchBp bp_norm{}, bp_sirt{};
   BatchFp fp{};
+  BpArgs a_norm{}, a_sirt{};  // the same work for the per-job kernels
+  double work = 0;            // remaining voxel-projection updates
   size_t smem_norm = 0, smem_sirt = 0;
   // progress
   JobState state = J_QUEUED;
@@ -117,6 +121,8 @@ struct tr_sched {
   std::thread worker;
   std::string err;
   tr_status fatal = TR_OK;
+  // TR_SCHED_BATCHED or TR_SCHED_SRPT
+  int policy = TR_SCHED_BATCHED;
   // counters
   long long steps = 0, items_bp = 0, items_fp = 0;
 };
@@ -202,10 +208,19 @@ FpArgs job_fp(const tr_sched *S, const Job &j, const float *vol, float *out) {
   return a;
 }
 
+size_t job_tiles(const Job &j) {
+  const dim3 g = bp_tile_grid(job_view(j, nullptr));
+  return (size_t)g.x * g.y * g.z;
+}
+
 // Device bytes a job holds while admitted.
 size_t job_bytes(const tr_sched *S, const Job &j) {
   const size_t p = j.plane, v = j.nvox;
-  size_t b = sizeof(TiltGeo) * j.d.ntilt + 2 * p * 4 + v * 4;  // geo, val, wt, wtvol
+  size_t b = sizeof(TiltGeo) * j.d.ntilt + p * 4;  // geo, val
+  if (j.d.sirt_iters > 0) {  // wt; compact voxel weights at their largest
+    const size_t tiles = job_tiles(j);
+    b += p * 4 + tiles * (kTileVox * 4 + 4) + 4 + (size_t)j.d.ny * 4;
+  }
   if (S->pdtype != TR_DTYPE_F32 || j.d.host) b += p * elem_size(S->pdtype);  // stored stack
   b += sizeof(float) * j.d.ntilt * 3;                        // scales, maxima (16-bit)
   if (S->rdtype != TR_DTYPE_F32) b += p * 2;                               // 16-bit residual
@@ -231,9 +246,10 @@ tr_status ensure_filter(tr_sched *S, int nx, std::pair<float2 *, float2 *> *out)
   const int M = 1 << sp.log2m;
   float2 *g = nullptr, *t = nullptr;
   SCHED_CUDA(S, cudaMalloc(&g, sizeof(float2) * M));
-  SCHED_CUDA(S, cudaMalloc(&t, sizeof(float2) * M));
+  SCHED_CUDA(S, cudaMalloc(&t, sizeof(float2) * sp.tw.size()));
   SCHED_CUDA(S, cudaMemcpy(g, sp.ghat.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
-  SCHED_CUDA(S, cudaMemcpy(t, sp.tw.data(), sizeof(float2) * M, cudaMemcpyHostToDevice));
+  SCHED_CUDA(S, cudaMemcpy(t, sp.tw.data(), sizeof(float2) * sp.tw.size(),
+                           cudaMemcpyHostToDevice));
   S->filt[nx] = {g, t};
   S->filt_h[nx] = sp;
   *out = {g, t};
@@ -260,10 +276,16 @@ tr_status admit(tr_sched *S, Job &j) {
     tr_status st = ensure_filter(S, j.d.nx, &filt);
     if (st) return st;
   }
+  const bool sirt = j.d.sirt_iters > 0;
+  const size_t tiles = job_tiles(j);
   SCHED_CUDA(S, alloc(&j.geo, sizeof(TiltGeo) * nt, ps));
   SCHED_CUDA(S, alloc(&j.val, P * 4, ps));
-  SCHED_CUDA(S, alloc(&j.wt, P * 4, ps));
-  SCHED_CUDA(S, alloc(&j.wtvol, V * 4, ps));
+  if (sirt) {
+    SCHED_CUDA(S, alloc(&j.wt, P * 4, ps));
+    SCHED_CUDA(S, alloc(&j.wslot, (tiles + 1) * sizeof(int), ps));
+    SCHED_CUDA(S, alloc(&j.wtvol, tiles * kTileVox * 4, ps));  // every tile a border tile
+    SCHED_CUDA(S, alloc(&j.wrow, (size_t)j.d.ny * 4, ps));
+  }
   if (j.pdtype != TR_DTYPE_F32 || j.d.host)
     SCHED_CUDA(S, alloc(&j.pstore, P * elem_size(j.pdtype), ps));
   if (j.pdtype != TR_DTYPE_F32) SCHED_CUDA(S, alloc(&j.pscale, sizeof(float) * nt, ps));
@@ -313,19 +335,31 @@ tr_status admit(tr_sched *S, Job &j) {
     SCHED_CUDA(S, cudaMemsetAsync(j.vol, 0, V * 4, ps));
   else if (j.d.host)
     SCHED_CUDA(S, cudaMemcpyAsync(j.vol_own, j.d.vol, V * 4, cudaMemcpyHostToDevice, ps));
-  // Geometry-only weights: splat of ones and the voxel sums of c.
-  SCHED_CUDA(S, cudaMemsetAsync(j.wt, 0, P * 4, ps));
-  SCHED_CUDA(S, launch_fp(j.gi.sep, job_fp(S, j, nullptr, j.wt), ps));
-  BpArgs w = job_bp(S, j, nullptr, TR_DTYPE_F32, nullptr, 1.f);
-  w.v.vol = j.wtvol;
-  w.out = j.wtvol;
-  w.err = nullptr;
-  SCHED_CUDA(S, launch_bp(BP_WEIGHTS, j.gi.sep, w, ps));
+  // Geometry-only weights of SIRT jobs: the splat of ones, and the voxel
+  // sums of c in compact form (tiles classified on the device; the border
+  // tiles' slots come from a device counter, so the worst-case buffer needs
+  // no read-back of the count).
+  if (sirt) {
+    SCHED_CUDA(S, cudaMemsetAsync(j.wt, 0, P * 4, ps));
+    SCHED_CUDA(S, launch_fp(j.gi.sep, job_fp(S, j, nullptr, j.wt), ps));
+    SCHED_CUDA(S, cudaMemsetAsync(j.wslot + tiles, 0, sizeof(int), ps));
+    SCHED_CUDA(S, launch_classify_tiles(j.geo, nt, job_view(j, nullptr), j.d.ox, j.d.oy, j.d.oz,
+                                        j.d.nx, j.d.ny, j.gi.sep, j.wslot, j.wslot + tiles, ps));
+    if (j.gi.sep)
+      SCHED_CUDA(S, launch_sep_row_weights(j.geo, nt, j.d.ny, j.d.oy, j.d.ny, j.wrow, ps));
+    BpArgs w = job_bp(S, j, nullptr, TR_DTYPE_F32, nullptr, 1.f);
+    w.v.vol = nullptr;
+    w.out = j.wtvol;
+    w.wslot = j.wslot;
+    w.err = nullptr;
+    SCHED_CUDA(S, launch_bp(BP_WEIGHTS, j.gi.sep, w, ps));
+  }
 
   // Step items (layouts fixed for the job's life).
   const dim3 gb = bp_tile_grid(job_view(j, j.vol)), gf = fp_tile_grid(job_view(j, j.vol));
   if (j.d.wbp) {
     BpArgs a = job_bp(S, j, j.val, TR_DTYPE_F32, nullptr, 1.f);
+    j.a_norm = a;
     if (!batch_bp_layout(a, j.gi.sep, S->smem_bp, &j.bp_norm, &j.smem_norm) ||
         j.smem_norm > S->smem_bp)
       return sched_fail(S, TR_ERR_UNSUPPORTED, "tile window does not suit the step's layout");
@@ -340,6 +374,10 @@ tr_status admit(tr_sched *S, Job &j) {
     const void *r = j.rdtype == TR_DTYPE_F32 ? (const void *)j.val : j.res;
     BpArgs a = job_bp(S, j, r, j.rdtype, j.rs, j.d.gamma);
     a.wtvol = j.wtvol;
+    a.wslot = j.wslot;
+    a.wrow = j.wrow;
+    a.wfull = (float)nt;
+    j.a_sirt = a;
     if (!batch_bp_layout(a, j.gi.sep, S->smem_bp, &j.bp_sirt, &j.smem_sirt) ||
         j.smem_sirt > S->smem_bp ||
         (size_t)j.fp.a.chunk * j.gi.fp_tilt_bytes > S->smem_fp)
@@ -357,12 +395,13 @@ tr_status admit(tr_sched *S, Job &j) {
 }
 
 void release(tr_sched *S, Job &j, cudaStream_t s) {
-  void *ptrs[] = {j.geo,    j.val, j.wt,     j.wtvol,  j.vol_own,
-                  j.pstore, j.res, j.pscale, j.rscale, j.maxbits};
+  void *ptrs[] = {j.geo,    j.val, j.wt,     j.wtvol,  j.vol_own, j.wrow,
+                  j.wslot,  j.pstore, j.res, j.pscale, j.rscale, j.maxbits};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, s);
   j.geo = nullptr;
-  j.val = j.wt = j.wtvol = j.vol_own = j.pscale = j.rscale = nullptr;
+  j.wslot = nullptr;
+  j.val = j.wt = j.wtvol = j.vol_own = j.pscale = j.rscale = j.wrow = nullptr;
   j.pstore = j.res = nullptr;
   j.maxbits = nullptr;
   S->used -= std::min(S->used, j.bytes);
@@ -402,10 +441,70 @@ tr_status configure(tr_sched *S, size_t smem_bp, int bp_per_sm) {
   return TR_OK;
 }
 
+double job_work(const Job &j) {
+  return ((j.wbp_pending ? 1.0 : 0.0) + 2.0 * j.iters_left) * j.d.ntilt * (double)j.nvox;
+}
+
+// TR_SCHED_SRPT step: the next unit of the ready job with the least remaining
+// work (its WBP back-projection, or one SIRT iteration) through the per-job
+// kernels the context path runs.  At most two steps are in flight, so a job
+// that becomes ready is considered within one step.
+tr_status launch_job_step(tr_sched *S, bool *launched) {
+  Job *j = nullptr;
+  for (auto &jp : S->active)
+    if (jp->state == J_READY && (jp->wbp_pending || jp->iters_left > 0) &&
+        (!j || job_work(*jp) < job_work(*j)))
+      j = jp.get();
+  if (!j) return TR_OK;
+  const int b = S->next_tab;
+  if (S->tab_used[b]) {
+    if (cudaEventQuery(S->tab_ev[b]) == cudaErrorNotReady) return TR_OK;  // try later
+    S->tab_used[b] = false;
+  }
+  cudaStream_t s = S->s;
+  if (j->wbp_pending) {
+    SCHED_CUDA(S, cudaMemsetAsync(S->err_d, 0, sizeof(int), s));
+    SCHED_CUDA(S, launch_bp(BP_NORM, j->gi.sep, j->a_norm, s));
+    j->wbp_pending = false;
+    ++S->items_bp;
+  } else {
+    const size_t plane = (size_t)j->d.nx * j->d.ny;
+    const int nt = j->d.ntilt;
+    SCHED_CUDA(S, cudaMemsetAsync(j->val, 0, j->plane * 4, s));
+    SCHED_CUDA(S, launch_fp(j->gi.sep, j->fp.a, s));
+    if (j->rdtype == TR_DTYPE_F16) {  // FP32 over val, then FP16 with own scales
+      SCHED_CUDA(S, launch_resid_lp(j->proj, j->pdtype, j->ps, j->val, j->wt, plane, nt,
+                                    TR_DTYPE_F32, j->val, nullptr, S->nsm, s));
+      SCHED_CUDA(S, launch_quantize(j->val, plane, nt, TR_DTYPE_F16, j->res, j->rscale,
+                                    j->maxbits, S->nsm, s));
+    } else {
+      void *r = j->rdtype == TR_DTYPE_F32 ? (void *)j->val : j->res;
+      SCHED_CUDA(S, launch_resid_lp(j->proj, j->pdtype, j->ps, j->val, j->wt, plane, nt,
+                                    j->rdtype, r, nullptr, S->nsm, s));
+    }
+    SCHED_CUDA(S, cudaMemsetAsync(S->err_d, 0, sizeof(int), s));
+    SCHED_CUDA(S, launch_bp(BP_SIRT, j->gi.sep, j->a_sirt, s));
+    --j->iters_left;
+    ++S->items_bp;
+    ++S->items_fp;
+  }
+  SCHED_CUDA(S, cudaEventRecord(S->tab_ev[b], s));
+  S->tab_used[b] = true;
+  S->next_tab = b ^ 1;
+  ++S->steps;
+  if (!j->wbp_pending && j->iters_left == 0) {
+    SCHED_CUDA(S, cudaEventRecord(j->ev_done, s));
+    j->state = J_DRAINING;
+  }
+  *launched = true;
+  return TR_OK;
+}
+
 // Builds and launches one step over the ready jobs (nothing when none has
 // work or the next table buffer is still being uploaded).
 tr_status launch_step(tr_sched *S, bool *launched) {
   *launched = false;
+  if (S->policy == TR_SCHED_SRPT) return launch_job_step(S, launched);
   std::vector<Job *> part;
   for (auto &jp : S->active)
     if (jp->state == J_READY && (jp->wbp_pending || jp->iters_left > 0)) part.push_back(jp.get());
@@ -505,14 +604,22 @@ tr_status launch_step(tr_sched *S, bool *launched) {
 // One pass of the scheduler (lock held): admit, advance, retire.
 tr_status progress(tr_sched *S, bool *busy) {
   *busy = false;
-  // Admit in order while the head fits.
+  // Admit while a job fits: the queue's head in order (TR_SCHED_BATCHED), or
+  // the queued job with the least work that fits (TR_SCHED_SRPT).  With
+  // nothing admitted, the chosen job is admitted whatever its size.
   while (!S->queue.empty()) {
-    Job &j = *S->queue.front();
+    auto pick = S->queue.begin();
+    if (S->policy == TR_SCHED_SRPT)
+      for (auto it = S->queue.begin(); it != S->queue.end(); ++it)
+        if (job_work(**it) < job_work(**pick) &&
+            (!S->budget || S->used + (*it)->bytes <= S->budget))
+          pick = it;
+    Job &j = **pick;
     if (S->budget && S->used + j.bytes > S->budget && !S->active.empty()) break;
     S->used += j.bytes;
     S->peak = std::max(S->peak, S->used);
-    S->active.push_back(S->queue.front());
-    S->queue.pop_front();
+    S->active.push_back(*pick);
+    S->queue.erase(pick);
     tr_status st = admit(S, j);
     if (st) return st;
     *busy = true;
@@ -655,6 +762,8 @@ tr_status tr_sched_submit(tr_sched *S, const tr_job *job, unsigned long long *id
   j->d.coeff8 = nullptr;
   j->plane = (size_t)d.nx * d.ny * d.ntilt;
   j->nvox = (size_t)d.nx * d.ny * d.thickness;
+  j->wbp_pending = d.wbp != 0;  // the work left, for the SRPT order while queued
+  j->iters_left = d.sirt_iters;
   std::vector<TiltGeo> g(d.ntilt);
   int bad = -1;
   const int gs = derive_geometry(j->coeff.data(), d.ntilt, d.nx, d.ny, d.thickness,
@@ -714,6 +823,13 @@ tr_status tr_sched_stats(tr_sched *S, tr_sched_info *out) {
 }
 
 const char *tr_sched_last_error(const tr_sched *S) { return S ? S->err.c_str() : "null"; }
+
+tr_status tr_sched_set_policy(tr_sched *S, int policy) {
+  if (!S || (policy != TR_SCHED_BATCHED && policy != TR_SCHED_SRPT)) return TR_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->policy = policy;
+  return TR_OK;
+}
 
 tr_status tr_sched_configure(tr_sched *S, size_t smem_bp, int bp_ctas_per_sm) {
   if (!S || smem_bp < 16 * 1024 || smem_bp > kSchedSmemMax || bp_ctas_per_sm < 0)

@@ -202,6 +202,37 @@ def project_series(engine, cfg: Config, layout: int = 0, noise: str = "gaussian"
     return proj.contiguous()
 
 
+def serve_stream(n: int, rate: float = 4.0, seed: int = 7):
+    """The serving configuration's request stream (seeded): Poisson arrivals
+    at ``rate`` per second; each request draws its series from the batched
+    configuration's distribution (projection size from {512^2, 1024^2,
+    2048^2}, tilt count from {41, 61, 81}, thickness U(64, 384)) and asks WBP,
+    SIRT-10 or SIRT-30 (uniform).  Returns (classes, requests): one phantom
+    series Config per (size, tilts) class, angles over +-U(60, 70) degrees,
+    whose projections every request of that class reconstructs at its own
+    thickness; requests are dicts (t, cls, thickness, method, iters)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    classes = {}
+    reqs = []
+    for k in range(n):
+        size = int(rng.choice([512, 1024, 2048]))
+        nt = int(rng.choice([41, 61, 81]))
+        th = int(rng.uniform(64, 384))
+        m = int(rng.integers(3))
+        key = (size, nt)
+        if key not in classes:
+            amax = float(rng.uniform(60.0, 70.0))
+            c = Config(f"serve{size}x{nt}", size, size, 256 * size // 2048,
+                       np.linspace(-amax, amax, nt).astype(np.float32), 50, 20,
+                       seed * 1000 + len(classes), offset_sigma=1.0, noise=0.1)
+            c.extra["scale"] = 256.0 / size
+            classes[key] = c
+        reqs.append(dict(t=float(t[k]), cls=key, thickness=th,
+                         method=["WBP", "SIRT-10", "SIRT-30"][m], iters=[0, 10, 30][m]))
+    return classes, reqs
+
+
 def batch_series(n: int = 64, seed: int = 3) -> list[Config]:
     """The batched configuration's tilt series (seeded): projection size
     drawn from {512^2, 1024^2, 2048^2}, tilt count from {41, 61, 81} over

@@ -105,6 +105,8 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_quantize.argtypes = [vp, vp, i, vp, vp, vp]
     lib.tr_backproject_lp.argtypes = [vp, vp, i, vp, vp, i, i, vp]
     lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
+    lib.tr_sirt_zslabs.argtypes = [vp, vp, i, vp, i, vp, i, i, f, i, vp]
+    lib.tr_autotune_zslab.argtypes = [vp, vp, i, vp, i, vp, i, C.POINTER(i), dp]
     lib.tr_synchronize.argtypes = [vp]
     lib.tr_selftest_wait.argtypes = [vp, i]
     for name in ("tr_create", "tr_destroy", "tr_set_problem", "tr_update_geometry",
@@ -311,6 +313,35 @@ class Engine:
                                         DTYPES[resid_dtype], _ptr(vol), iters, gamma,
                                         _stream(self.device)), "tr_sirt_lp")
 
+    @staticmethod
+    def _slab_vol(vol):
+        """(pointer, on_host) of a z-slab volume: a CUDA tensor, or host
+        memory (a CPU tensor, page-locked for overlapped copies, or a float32
+        C-contiguous numpy array)."""
+        if isinstance(vol, np.ndarray):
+            assert vol.dtype == np.float32 and vol.flags.c_contiguous
+            return vol.ctypes.data, 1
+        assert vol.is_contiguous()
+        return vol.data_ptr(), 0 if vol.is_cuda else 1
+
+    def sirt_zslabs(self, proj, vol, iters, gamma, depth, scale=None, resid_dtype="f32"):
+        """tr_sirt_zslabs: SIRT over z-slabs of `depth` sections; `vol` on
+        the device or host-resident (see :meth:`_slab_vol`); proj FP32 or a
+        16-bit stack with its scales."""
+        vp, host = self._slab_vol(vol)
+        self._check(self.lib.tr_sirt_zslabs(self.h, _ptr(proj), _dtype_code(proj), _ptr(scale),
+                                            DTYPES[resid_dtype], vp, host, iters, gamma, depth,
+                                            _stream(self.device)), "tr_sirt_zslabs")
+
+    def autotune_zslab(self, proj, vol, scale=None, resid_dtype="f32"):
+        """tr_autotune_zslab: (slab depth, sweep ms)."""
+        vp, host = self._slab_vol(vol)
+        d, ms = C.c_int(), C.c_double()
+        self._check(self.lib.tr_autotune_zslab(self.h, _ptr(proj), _dtype_code(proj),
+                                               _ptr(scale), DTYPES[resid_dtype], vp, host,
+                                               C.byref(d), C.byref(ms)), "tr_autotune_zslab")
+        return d.value, ms.value
+
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")
 
@@ -411,6 +442,7 @@ class Scheduler:
         L.tr_sched_last_error.argtypes = [vp]
         L.tr_sched_last_error.restype = C.c_char_p
         L.tr_sched_configure.argtypes = [vp, sz, i]
+        L.tr_sched_set_policy.argtypes = [vp, i]
         L.tr_sched_autotune.argtypes = [vp, C.POINTER(Job), i, C.POINTER(sz), C.POINTER(i)]
         L.tr_sched_destroy.argtypes = [vp]
         h = vp()
@@ -469,6 +501,13 @@ class Scheduler:
     def configure(self, smem_bp: int, bp_ctas_per_sm: int = 0):
         self._check(self.lib.tr_sched_configure(self.h, smem_bp, bp_ctas_per_sm),
                     "tr_sched_configure")
+
+    def set_policy(self, policy: str):
+        """'batched' (all admitted jobs per step, persistent graph-replayed
+        launches) or 'srpt' (shortest remaining work first, per-job
+        kernels)."""
+        self._check(self.lib.tr_sched_set_policy(self.h, {"batched": 0, "srpt": 1}[policy]),
+                    "tr_sched_set_policy")
 
     def autotune(self, probe: Job, iters: int = 2):
         sm, ct = C.c_size_t(), C.c_int()

@@ -419,10 +419,18 @@ def run_kernels(args):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / max(1, args.iters)
+    # One R-weighting filter of the stack (the WBP filter) after the SIRT
+    # iterations, on a copy.
+    filt = proj.clone()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    eng.filter_rweight(filt)
+    f1.record()
+    torch.cuda.synchronize()
     print(json.dumps({"case": f"cfg1/{args.scale}" + (" separable" if args.separable else ""),
                       "proj": [nt, ny, nx],
                       "volume": [nx, ny, th], "iters": args.iters,
-                      "ms_per_iter": ms}), flush=True)
+                      "ms_per_iter": ms, "rweight_ms": f0.elapsed_time(f1)}), flush=True)
     eng.close()
 
 
@@ -544,6 +552,24 @@ def run_cfg2(args):
     t_lp = timed(lambda: eng.sirt_lp(q, scale, vol, iters, cfg.gamma, "f16"))
     lp_band = vol[:, r0:r0 + band].cpu().numpy()
     p_band = proj[:, r0:r0 + band].cpu().numpy()
+    # The same FP16 SIRT through z-slabs: the volume host-resident (page-locked)
+    # and streamed through three device slabs at the autotuned depth, then the
+    # device-resident volume swept slab by slab at that depth.
+    del vol
+    torch.cuda.empty_cache()
+    hvol = torch.zeros((th, ny, nx), pin_memory=True)
+    depth, sweep_ms = eng.autotune_zslab(q, hvol, scale, "f16")
+    hvol.zero_()
+    t0 = time.perf_counter()
+    eng.sirt_zslabs(q, hvol, iters, cfg.gamma, depth, scale, "f16")
+    t_host = time.perf_counter() - t0
+    host_band = hvol[:, r0:r0 + band].numpy().copy()
+    del hvol
+    dvol = torch.zeros((th, ny, nx), device="cuda")
+    vol = dvol
+    t_dev = timed(lambda: eng.sirt_zslabs(q, dvol, iters, cfg.gamma, depth, scale, "f16"))
+    dev_band = dvol[:, r0:r0 + band].cpu().numpy()
+    del dvol, vol
     eng.close()
     R = oracle.Restatement()
     g = R.geom(nx, band, nt, th, T.LAYOUT_Z, 0, (org[0], org[1] - r0, org[2]))
@@ -562,6 +588,11 @@ def run_cfg2(args):
                       "vs_fp64_oracle": err(lp_band),
                       "plain_f32": {"value": vpu / t_f32, "seconds": t_f32,
                                     "vs_fp64_oracle": err(f32_band)},
+                      "zslab": {"depth": depth, "autotune_sweep_ms": sweep_ms,
+                                "host_resident": {"value": vpu / t_host, "seconds": t_host,
+                                                  "vs_fp64_oracle": err(host_band)},
+                                "device_resident": {"value": vpu / t_dev, "seconds": t_dev,
+                                                    "vs_fp64_oracle": err(dev_band)}},
                       "oracle": {"rows": [r0, r0 + band], "seconds": oracle_s},
                       "generation_s": gen_s, "data": "synthetic",
                       "config": {"method": f"SIRT-{iters}", "tilts": nt, "proj": [ny, nx],
@@ -701,12 +732,19 @@ def run_batch(args):
 
 
 def run_serve(args):
-    """Serving configuration: Poisson arrivals of jobs drawn from the batched
-    configuration's series (host buffers in, host volume out), methods uniform
-    over WBP, SIRT-10, SIRT-30.  The scheduler (continuous batching under the
-    HBM budget, 16-bit storage) and the plain GPU form (one job at a time
-    through tr_reconstruct_host, FP32, FIFO) see the same arrival times; both
-    report p50/p99 latency from arrival to the volume in host memory."""
+    """Serving configuration: a seeded Poisson stream (rate --rate, default 4
+    per second; seed 7) of --jobs requests (default 200: a prefix of the
+    2000-request stream), each drawn from the batched configuration's series
+    distribution and asking WBP, SIRT-10 or SIRT-30; host buffers in, host
+    volume out, 150 GB HBM budget.  Forms, each fed the same arrivals:
+      * plain: one request at a time in arrival order through
+        tr_reconstruct_host (FP32), a FIFO single server;
+      * the scheduler (16-bit storage) under each step policy, fed by a
+        front end that keeps --inflight requests submitted (the shortest
+        pending one next under SRPT, the oldest under the batched policy).
+    Latency runs from arrival to the volume in host memory.  Each request's
+    middle volume row from the scheduler is compared with the plain FP32
+    result (relative L2)."""
     import threading as th
 
     import torch
@@ -715,92 +753,151 @@ def run_serve(args):
     from autom2_b200 import tiltrec as T
     build.build_lib()
     torch.cuda.set_device(0)
-    rng = np.random.default_rng(7)
-    pool_specs = synth.batch_series(args.series, seed=7)
+    n = args.jobs or 200
+    rate = args.rate or 4.0
+    classes, reqs = synth.serve_stream(n, rate, seed=7)
     eng = T.Engine(0)
-    series = []
-    for c in pool_specs:
+    series = {}
+    t0 = time.perf_counter()
+    for key, c in classes.items():
         c8 = synth.coefficients(c)
         eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
         p = synth.project_series(eng, c, 0, "gaussian").cpu().pin_memory()
-        out = torch.zeros((c.ny, c.thickness, c.nx)).pin_memory()
-        series.append((c, c8, p.numpy(), out.numpy(), p, out))
-    methods = [("WBP", True, 0), ("SIRT-10", False, 10), ("SIRT-30", False, 30)]
-    njobs = args.jobs or 64
-    jobs = [(int(rng.integers(len(series))), methods[int(rng.integers(3))]) for _ in range(njobs)]
-    mean_vpu = float(np.mean([job_vpu(series[s][0], m[1], m[2]) for s, m in jobs]))
-    rate = args.rate
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, njobs))
-    busy = [th.Lock() for _ in series]  # one output buffer per series
+        series[key] = (c, c8, p)
+    gen_s = time.perf_counter() - t0
+    K = args.inflight
+    sizes = sorted({key[0] for key in classes})
+    bufs = {s: [torch.empty(s * s * 384).pin_memory() for _ in range(K)] for s in sizes}
 
-    def run_form(submit_fn):
-        lat = [0.0] * njobs
-        done_at = [0.0] * njobs
+    def work(k):
+        r = reqs[k]
+        c = series[r["cls"]][0]
+        return (int(r["iters"] == 0) + 2 * r["iters"]) * c.ntilt * c.nx * c.ny * r["thickness"]
+
+    mean_vpu = float(np.mean([work(k) for k in range(n)]))
+
+    def out_view(buf, c, thk):
+        return buf[: c.ny * thk * c.nx].view(c.ny, thk, c.nx)
+
+    def serve(run_one, order, limit):
+        """Feeds arrivals to `run_one(k, buf, finish)` with at most `limit`
+        in flight; returns latencies, makespan, middle rows."""
+        lock = th.Condition()
+        pending, done_at, rows = [], [0.0] * n, [None] * n
+        state = {"inflight": 0, "next": 0}
+        free = {s: list(bufs[s]) for s in sizes}
+        start = time.perf_counter()
+
+        def finish(k, buf):
+            c = series[reqs[k]["cls"]][0]
+            done_at[k] = time.perf_counter() - start
+            rows[k] = out_view(buf, c, reqs[k]["thickness"])[c.ny // 2].numpy().copy()
+            with lock:
+                free[c.nx].append(buf)
+                state["inflight"] -= 1
+                lock.notify_all()
+
         threads = []
-        t0 = time.perf_counter()
-
-        def one(k):
-            s, m = jobs[k]
-            delay = t0 + arrivals[k] - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            with busy[s]:
-                submit_fn(s, m)
-                done_at[k] = time.perf_counter()
-            lat[k] = done_at[k] - (t0 + arrivals[k])
-
-        for k in range(njobs):
-            t = th.Thread(target=one, args=(k,))
-            t.start()
-            threads.append(t)
+        for _ in range(n):
+            with lock:
+                while True:
+                    now = time.perf_counter() - start
+                    while state["next"] < n and reqs[state["next"]]["t"] <= now:
+                        pending.append(state["next"])
+                        state["next"] += 1
+                    if pending and state["inflight"] < limit:
+                        break
+                    wait = 0.05
+                    if state["next"] < n:
+                        wait = min(wait, max(0.0, reqs[state["next"]]["t"] - now))
+                    lock.wait(timeout=wait)
+                k = min(pending, key=work) if order == "srpt" else pending[0]
+                pending.remove(k)
+                state["inflight"] += 1
+                buf = free[series[reqs[k]["cls"]][0].nx].pop()
+            t = run_one(k, buf, finish)
+            if t is not None:
+                threads.append(t)
         for t in threads:
             t.join()
-        return lat, max(done_at) - t0
+        lat = [done_at[k] - reqs[k]["t"] for k in range(n)]
+        return lat, max(done_at), rows
 
-    # plain: one job at a time in arrival order (a FIFO single server)
-    fifo = th.Lock()
+    # plain: FIFO single server, one request at a time
+    def plain_one(k, buf, finish):
+        r = reqs[k]
+        c, c8, p = series[r["cls"]]
+        eng.set_problem(c.nx, c.ny, c.ntilt, r["thickness"], c8, T.LAYOUT_Y)
+        v = out_view(buf, c, r["thickness"])
+        eng.reconstruct_host("WBP" if r["iters"] == 0 else "SIRT", p.numpy(), v.numpy(),
+                             r["iters"], 0.5, zero_start=True)
+        finish(k, buf)
+        return None
 
-    def plain_submit(s, m):
-        c, c8, pnp, onp, _, _ = series[s]
-        with fifo:
-            eng.set_problem(c.nx, c.ny, c.ntilt, c.thickness, c8, T.LAYOUT_Y)
-            eng.reconstruct_host("WBP" if m[1] else "SIRT", pnp, onp, m[2], 0.5,
-                                 zero_start=True)
-
-    lat_plain, span_plain = run_form(plain_submit)
+    lat_p, span_p, rows_p = serve(plain_one, "fifo", 1)
     eng.close()
-    free, _ = torch.cuda.mem_get_info()
-    budget = min(int(args.budget_gb * 1e9), int(free - 8e9))
-    S = T.Scheduler(0, hbm_budget=budget, proj_dtype=args.storage, resid_dtype=args.storage)
+    free_b, _ = torch.cuda.mem_get_info()
+    budget = min(int(args.budget_gb * 1e9), int(free_b - 8e9))
+    forms = {}
+    for policy in ("srpt", "batched"):
+        S = T.Scheduler(0, hbm_budget=budget, proj_dtype=args.storage, resid_dtype=args.storage)
+        S.set_policy(policy)
 
-    def sched_submit(s, m):
-        c, c8, pnp, onp, _, _ = series[s]
-        S.wait(S.submit(S.job(pnp, onp, c8, T.LAYOUT_Y, wbp=m[1], sirt_iters=m[2],
-                              gamma=0.5)))
+        def sched_one(k, buf, finish, S=S):
+            r = reqs[k]
+            c, c8, p = series[r["cls"]]
+            v = out_view(buf, c, r["thickness"])
+            jid = S.submit(S.job(p.numpy(), v.numpy(), c8, T.LAYOUT_Y, wbp=r["iters"] == 0,
+                                 sirt_iters=r["iters"], gamma=0.5))
 
-    lat_s, span_s = run_form(sched_submit)
-    info = S.stats()
-    S.close()
+            def waiter():
+                S.wait(jid)
+                finish(k, buf)
+            t = th.Thread(target=waiter)
+            t.start()
+            return t
 
-    def pct(x, q):
-        return float(np.percentile(np.asarray(x), q))
-
+        lat, span, rows = serve(sched_one, policy, K)
+        info = S.stats()
+        S.close()
+        errs = [oracle_free_rel_l2(a, b) for a, b in zip(rows, rows_p)]
+        forms[policy] = {"value": n / span * 3600, "makespan_s": span,
+                         "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
+                         "mean_latency_s": float(np.mean(lat)),
+                         "rel_l2_vs_plain_f32_middle_row": {"max": max(errs),
+                                                            "median": pct(errs, 50)},
+                         "scheduler": info}
+    best = forms["srpt"]
     line = {"workload": "serve", "metric": "reconstructions/hour", "unit": "recon/h",
-            "value": njobs / span_s * 3600, "higher_is_better": True, "n_gpus": 1,
-            "jobs": njobs, "arrival_rate_per_s": rate,
-            "offered_vpu_per_s": mean_vpu * rate,
-            "p50_latency_s": pct(lat_s, 50), "p99_latency_s": pct(lat_s, 99),
-            "makespan_s": span_s, "dtype": f"{args.storage} storage, f32 accumulate",
-            "plain": {"value": njobs / span_plain * 3600, "p50_latency_s": pct(lat_plain, 50),
-                      "p99_latency_s": pct(lat_plain, 99), "makespan_s": span_plain,
-                      "form": "FIFO, one job at a time through tr_reconstruct_host, f32"},
-            "speedup_vs_plain": span_plain / span_s, "scheduler": info,
-            "data": "synthetic", "config": {
-                "series_pool": args.series, "methods": "uniform WBP / SIRT-10 / SIRT-30",
-                "host_buffers": "pinned", "budget_bytes": budget,
-                "note": "one output buffer per series: a job waits for it while a job of "
-                        "the same series is in flight (counted in its latency)"}}
+            "value": best["value"], "higher_is_better": True, "n_gpus": 1,
+            "jobs": n, "arrival_rate_per_s": rate, "offered_vpu_per_s": mean_vpu * rate,
+            "p50_latency_s": best["p50_latency_s"], "p99_latency_s": best["p99_latency_s"],
+            "makespan_s": best["makespan_s"],
+            "dtype": f"{args.storage} storage, f32 accumulate",
+            "speedup_vs_plain": span_p / best["makespan_s"],
+            "p50_latency_ratio_plain_over_srpt": pct(lat_p, 50) / best["p50_latency_s"],
+            "plain": {"value": n / span_p * 3600, "p50_latency_s": pct(lat_p, 50),
+                      "p99_latency_s": pct(lat_p, 99), "mean_latency_s": float(np.mean(lat_p)),
+                      "makespan_s": span_p,
+                      "form": "FIFO, one request at a time through tr_reconstruct_host, f32"},
+            "scheduler_forms": forms, "generation_s": gen_s, "data": "synthetic",
+            "config": {"stream": f"Poisson {rate}/s, seed 7, first {n} of the 2000-request "
+                                 "stream", "series": "N in {512,1024,2048}, T in {41,61,81} "
+                                 "over +-U(60,70) deg, th U(64,384)",
+                       "methods": "uniform WBP / SIRT-10 / SIRT-30 (0.5)",
+                       "host_buffers": "pinned", "budget_bytes": budget,
+                       "inflight": K, "error": "rel-L2 of each request's middle row vs the "
+                       "plain FP32 result (an FP64 oracle is out of reach at these sizes)"}}
     print(json.dumps(line), flush=True)
+
+
+def pct(x, q):
+    return float(np.percentile(np.asarray(x), q))
+
+
+def oracle_free_rel_l2(a, b):
+    a64, b64 = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a64 - b64) / max(np.linalg.norm(b64), 1e-300))
 
 
 def main():
@@ -820,8 +917,10 @@ def main():
                     help="sirt: the headline SIRT-30 line; batch / serve: the batched "
                          "and serving configurations (one JSON line each)")
     ap.add_argument("--jobs", type=int, default=0)
-    ap.add_argument("--series", type=int, default=12)
-    ap.add_argument("--rate", type=float, default=1.0, help="serve: arrivals per second")
+    ap.add_argument("--rate", type=float, default=0.0,
+                    help="serve: arrivals per second (default 4)")
+    ap.add_argument("--inflight", type=int, default=4,
+                    help="serve: requests the front end keeps submitted")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--storage", default="f16", choices=["f32", "f16", "bf16"])
     args = ap.parse_args()

@@ -242,17 +242,54 @@ tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
                      const float *scale_dev, int resid_dtype, float *vol_dev,
                      int iters, float gamma, void *stream);
 
+/* SIRT over z-slabs (TiltRecZ's split of the volume along z,
+ * TR/main/main-mpiz.cpp:1054-1069, with CuSIRTZ's iteration,
+ * TR/TiltRec_cuda_z/recon_z.cu:85-190), either layout, storage as
+ * tr_sirt_lp.  Each iteration is one sweep over the slabs: the SIRT update of
+ * slab k from the residual, then the forward projection of the updated slab
+ * into the next iteration's sums, so every slab is touched once per
+ * iteration.  vol_on_host != 0: `vol` is host memory (page-locked for the
+ * copies to overlap; any size the host holds) staged through three device
+ * slabs, slab k+1 copied in and slab k-1 copied out while slab k computes;
+ * the call then returns when the volume is written back.  Otherwise `vol` is
+ * the device volume and the call is ordered on `stream`.  depth: sections per
+ * slab, rounded down to a multiple of 32 (at least 32; the whole thickness
+ * when larger).  Results equal tr_sirt / tr_sirt_lp up to the order of the
+ * forward projection's float atomic adds.  Device memory: two reprojections
+ * (ntilt*ny*nx floats each), the weights, and with a host volume three slabs
+ * of depth*ny*nx floats. */
+tr_status tr_sirt_zslabs(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
+                         const float *scale_dev, int resid_dtype, float *vol,
+                         int vol_on_host, int iters, float gamma, int depth,
+                         void *stream);
+
+/* Picks the slab depth for tr_sirt_zslabs: times one full sweep (copies,
+ * update with gamma 0 over a zero residual, forward projection; the volume's
+ * values are unchanged) at depths 32, 64, 128, 256, 512 (those that fit the
+ * HBM budget) and returns the fastest, with its sweep time in ms when
+ * sweep_ms is not NULL.  Blocking. */
+tr_status tr_autotune_zslab(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
+                            const float *scale_dev, int resid_dtype, float *vol,
+                            int vol_on_host, int *depth_out, double *sweep_ms);
+
 /* ---- Batched jobs and serving.  No counterpart in the reference, which
  * reconstructs one tilt series per process run.
  *
  * A scheduler owns one device and an HBM budget.  Submitted jobs are
- * admitted in order while their device memory fits the budget; admission
- * (upload, 16-bit storage of the projections, WBP filtering, weights)
- * overlaps the running jobs.  All admitted jobs advance together, one step at
- * a time: a step is one persistent forward-projection launch, one residual
- * launch and one persistent back-projection launch over the tiles of every
- * job (a WBP back-projection or one SIRT iteration each), replayed from a
- * CUDA graph.  A background thread drives the steps; calls are thread-safe.
+ * admitted while their device memory fits the budget; admission (upload,
+ * 16-bit storage of the projections, WBP filtering, the weights of SIRT
+ * jobs) runs on its own stream and overlaps the running jobs, and a finished
+ * job's volume is copied back on a third.  Two step policies:
+ *  - TR_SCHED_BATCHED (default): jobs are admitted in submission order and
+ *    all admitted jobs advance together, one step at a time: a step is one
+ *    persistent forward-projection launch, one residual launch and one
+ *    persistent back-projection launch over the tiles of every job (a WBP
+ *    back-projection or one SIRT iteration each), replayed from a CUDA graph.
+ *  - TR_SCHED_SRPT: shortest remaining work first.  Admission takes the
+ *    queued job with the least work that fits; each step runs the next unit
+ *    (WBP back-projection or SIRT iteration) of the ready job with the least
+ *    work left, through the same per-job kernels as tr_sirt / tr_wbp.
+ * A background thread drives the steps; calls are thread-safe.
  * Results do not depend on the other jobs in the mix beyond the order of the
  * forward projection's float atomic adds (as for a job run alone).  Images
  * must suit the TMA staging: rows of a multiple of 16 bytes (nx % 4 == 0 for
@@ -298,6 +335,11 @@ const char *tr_sched_last_error(const tr_sched *s);
 /* Launch configuration of the steps (waits until idle): back-projection
  * shared-memory budget per CTA and resident CTAs per SM (0: as many as fit). */
 tr_status tr_sched_configure(tr_sched *s, size_t smem_bp, int bp_ctas_per_sm);
+#define TR_SCHED_BATCHED 0
+#define TR_SCHED_SRPT 1
+/* Step policy (TR_SCHED_BATCHED / TR_SCHED_SRPT); takes effect at the next
+ * step or admission. */
+tr_status tr_sched_set_policy(tr_sched *s, int policy);
 /* Autotuner: times `iters` SIRT steps of a device-resident probe job (run on
  * a scratch copy of its volume) under candidate configurations -- shared
  * memory per back-projection CTA (40, 56, 80, 112 KiB) at full residency,

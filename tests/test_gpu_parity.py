@@ -188,7 +188,10 @@ def test_zslabs_add_up(engine, restatement, layout):
     assert O.rel_l2(host(summed), host(whole)) < 2e-5
 
 
-@pytest.mark.parametrize("nx", [256, 1024, 4096])
+# FFT sizes M = 16 .. 16384: every first-pass radix (2, 4, 8, none), the
+# two-butterfly blocks of M = 16384, and an odd row count (9) so the last
+# pair has one row.
+@pytest.mark.parametrize("nx", [8, 12, 40, 100, 256, 500, 1024, 4096, 7000])
 def test_filter_widths(engine, restatement, nx):
     rng = np.random.default_rng(nx)
     rows = rng.normal(size=(1, 9, nx)).astype(np.float32)

@@ -123,9 +123,16 @@ def test_batch_fp16_storage_vs_fp64(engine, restatement):
 def test_budget_admission(engine, restatement):
     R = restatement
     jobs = _jobs(R, n=4, seed=2)
-    # device job bytes: geometry + val + wt (8 B/pixel) + voxel weights (4 B/voxel)
-    need = [112 * j["nt"] + 8 * j["nt"] * j["ny"] * j["nx"] + 4 * j["nx"] * j["ny"] * j["th"]
-            for j in jobs]
+    # device job bytes: geometry + val (4 B/pixel); SIRT jobs also wt (4 B/pixel)
+    # and compact voxel weights at their largest (a slot and 32x4x32 weights
+    # per tile, the border count, a weight per row)
+    def need_of(j):
+        tiles = -(-j["nx"] // 32) * -(-j["ny"] // 4) * -(-j["th"] // 32)
+        b = 112 * j["nt"] + 4 * j["nt"] * j["ny"] * j["nx"]
+        if j["iters"]:
+            b += 4 * j["nt"] * j["ny"] * j["nx"] + tiles * (4096 * 4 + 4) + 4 + 4 * j["ny"]
+        return b
+    need = [need_of(j) for j in jobs]
     budget = max(need) + min(need) // 2
     S = T.Scheduler(0, hbm_budget=budget)
     try:
@@ -155,5 +162,80 @@ def test_autotune_picks_a_candidate(engine, restatement):
         assert float(v.abs().sum()) == 0.0  # the probe ran on a copy of its volume
         got, _ = _run(S, [j])
         assert O.rel_l2(got[0], _oracle(R, j)) < 1e-5
+    finally:
+        S.close()
+
+
+@pytest.mark.parametrize("policy", ["batched", "srpt"])
+def test_jobs_admitted_while_another_is_mid_iteration(engine, restatement, policy):
+    """Continuous batching: a long SIRT job is already stepping when two more
+    jobs arrive; they are admitted while it runs, run alongside it (batched)
+    or ahead of it (shortest remaining work first), finish before it, and
+    each result equals the job run alone (1e-6: only the forward projection's
+    float atomic order differs) and the oracle (1e-5)."""
+    import time
+    R = restatement
+    rng = np.random.default_rng(17)
+    jobs = []
+    for k, (nx, ny, nt, th, iters) in enumerate([(128, 40, 13, 20, 150), (96, 24, 9, 12, 2),
+                                                (64, 40, 13, 8, 3)]):
+        ang = np.linspace(-60, 60, nt).astype(np.float32)
+        c8 = R.coeffs(ang, 0.5, 1.0 if k == 0 else 0.0, 0.0)
+        jobs.append(dict(nx=nx, ny=ny, nt=nt, th=th, layout=k % 2, c8=c8,
+                         proj=rng.normal(size=(nt, ny, nx)).astype(np.float32),
+                         wbp=k == 2, iters=iters, gamma=0.5))
+    S = T.Scheduler(0)
+    S.set_policy(policy)
+    try:
+        keep, ids, t_sub = [], [], []
+
+        def submit(j):
+            p = torch.from_numpy(j["proj"]).cuda()
+            v = torch.zeros(_vshape(j), device="cuda")
+            keep.append((p, v))
+            t_sub.append(time.perf_counter())
+            ids.append(S.submit(S.job(p, v, j["c8"], j["layout"], wbp=j["wbp"],
+                                      sirt_iters=j["iters"], gamma=j["gamma"])))
+
+        submit(jobs[0])
+        t0 = time.perf_counter()
+        while S.stats()["steps"] < 3:  # the long job is iterating
+            assert time.perf_counter() - t0 < 60, "the long job never started"
+            time.sleep(0.001)
+        steps_at_arrival = S.stats()["steps"]
+        submit(jobs[1])
+        submit(jobs[2])
+        done = [t + S.wait(i) for t, i in zip(t_sub, ids)]
+        assert steps_at_arrival < jobs[0]["iters"]  # arrived mid-iteration
+        assert done[1] < done[0] and done[2] < done[0]  # ran alongside the long job
+        mixed = [v.cpu().numpy() for _, v in keep]
+        for j, got in zip(jobs, mixed):
+            alone, _ = _run(S, [j])
+            assert O.rel_l2(got, alone[0]) < 1e-6
+            assert O.rel_l2(got, _oracle(R, j)) < 1e-5
+    finally:
+        S.close()
+
+
+def test_srpt_policy_matches_oracle_and_orders_by_work(engine, restatement):
+    """Shortest remaining work first: the same results as the oracle and as the
+    batched steps, every job submitted at once.  (The order by work is
+    checked with a long job in test_jobs_admitted_while_another_is_mid_iteration:
+    jobs this small finish within their neighbours' admission.)"""
+    R = restatement
+    jobs = _jobs(R, n=6, seed=21)
+    S = T.Scheduler(0)
+    S.set_policy("srpt")
+    try:
+        got, lat = _run(S, jobs)
+        for j, v in zip(jobs, got):
+            assert O.rel_l2(v, _oracle(R, j)) < 1e-5
+        work = [(int(j["wbp"]) + 2 * j["iters"]) * j["nt"] * j["nx"] * j["ny"] * j["th"]
+                for j in jobs]
+        assert all(x > 0 for x in lat) and len(set(work)) > 1
+        S.set_policy("batched")
+        again, _ = _run(S, jobs)
+        for a, b in zip(got, again):
+            assert O.rel_l2(a, b) < 1e-6
     finally:
         S.close()
