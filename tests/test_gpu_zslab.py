@@ -103,7 +103,7 @@ def test_zslab_budget_limits_depth(restatement):
     try:  # scratch of a 32-section run, measured
         probe.set_problem(nx, ny, nt, th, c8, 1, org)
         probe.sirt_zslabs(p, torch.from_numpy(vol0).pin_memory(), 1, 0.5, 32)
-        need32 = probe.scratch_bytes()
+        need32 = probe.scratch_bytes
     finally:
         probe.close()
     e = T.Engine(0, hbm_budget=need32 + 48 * section)  # 64 needs 96 more sections
