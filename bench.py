@@ -48,12 +48,14 @@ def peaks():
 
 
 # DRAM bytes per full cfg1 launch of the dominant kernels, from one ncu
-# capture each (dram__bytes_read.sum + dram__bytes_write.sum of a 512^2 x 61,
-# 512^2 x 128 case, scaled by component to the full launch: voxel-side bytes
-# x 8, detector-side bytes x 4).  The captures, their commands and the
-# scaling are summarised in profiles/fp_kernel.md and profiles/bp_kernel.md;
-# None where no capture of the current kernel exists yet.
-TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": None, "bp_kernel": None}
+# capture each (dram__bytes_read.sum + dram__bytes_write.sum of the cfg1
+# geometry at half the lengths: stack 61 x 512^2, volume 512^2 x 128), scaled
+# by component to the full launch: voxel-side bytes x 8, detector-side bytes
+# x 4.  fp_kernel: 134.2 MB volume read x 8 + (66.7 MB read + 67.4 MB
+# written) x 4; bp_tma_kernel (SIRT): (134.2 MB volume read + 110.3 MB
+# written) x 8 + 240.4 MB detector-side reads x 4.  The captures and their
+# commands are summarised in profiles/fp_kernel.md and profiles/bp_kernel.md.
+TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": 1.6100e9, "bp_kernel": 2.9173e9}
 
 
 class ClockSampler:
