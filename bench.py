@@ -686,37 +686,46 @@ def run_batch(args):
     pv = torch.zeros((c.ny, c.thickness, c.nx), device="cuda")
     tuned = S.autotune(S.job(proj, pv, c8, T.LAYOUT_Y, sirt_iters=2, gamma=c.gamma))
     del pv
-    results = {}
-    lat = [0.0] * len(series)
-    errs = []
     import threading as th
 
-    def waiter(i, jid, key, b):
-        lat[i] = S.wait(jid)
-        if i in cmp_idx:
-            results[i] = vol_for(b, series[i][0]).clone()
-        pool.give(key, b)
+    def run_sched():
+        results = {}
+        lat = [0.0] * len(series)
 
-    threads = []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for i, (c, c8, proj) in enumerate(series):
-        b = pool.take(c.nx)
-        v = vol_for(b, c)
-        jid = S.submit(S.job(proj, v, c8, T.LAYOUT_Y, wbp=True, sirt_iters=c.iters,
-                             gamma=c.gamma))
-        t = th.Thread(target=waiter, args=(i, jid, c.nx, b))
-        t.start()
-        threads.append(t)
-    for t in threads:
-        t.join()
-    torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
+        def waiter(i, jid, key, b):
+            try:
+                lat[i] = S.wait(jid)
+                if i in cmp_idx:
+                    results[i] = vol_for(b, series[i][0]).clone()
+            finally:
+                pool.give(key, b)
+
+        threads = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i, (c, c8, proj) in enumerate(series):
+            b = pool.take(c.nx)
+            v = vol_for(b, c)
+            jid = S.submit(S.job(proj, v, c8, T.LAYOUT_Y, wbp=True, sirt_iters=c.iters,
+                                 gamma=c.gamma))
+            t = th.Thread(target=waiter, args=(i, jid, c.nx, b))
+            t.start()
+            threads.append(t)
+        for t in threads:
+            t.join()
+        torch.cuda.synchronize()
+        span = time.perf_counter() - t0
+        errs = []
+        for i in cmp_idx:
+            a, r = results[i].double(), plain_ref[i].double()
+            errs.append(float((a - r).norm() / r.norm()))
+        return span, lat, errs
+
+    t_batch, lat, errs = run_sched()
     info = S.stats()
+    S.set_policy("srpt")
+    t_srpt, lat_srpt, errs_srpt = run_sched()
     S.close()
-    for i in cmp_idx:
-        a, r = results[i].double(), plain_ref[i].double()
-        errs.append(float((a - r).norm() / r.norm()))
     line = {"workload": "batch", "metric": "voxel-proj updates/s", "unit": "VPU/s",
             "value": total_vpu / t_batch, "n_gpus": 1, "higher_is_better": True,
             "jobs": len(series), "recon_per_hour": len(series) / t_batch * 3600,
@@ -728,6 +737,14 @@ def run_batch(args):
             "rel_l2_vs_plain_f32": {"max": max(errs), "jobs": cmp_idx},
             "p50_latency_s": statistics.median(lat), "autotune": {"smem_bp": tuned[0],
                                                                    "ctas_per_sm": tuned[1]},
+            "srpt": {"value": total_vpu / t_srpt, "seconds": t_srpt,
+                     "recon_per_hour": len(series) / t_srpt * 3600,
+                     "speedup_vs_plain": t_plain / t_srpt,
+                     "p50_latency_s": statistics.median(lat_srpt),
+                     "mean_latency_s": float(np.mean(lat_srpt)),
+                     "rel_l2_vs_plain_f32_max": max(errs_srpt),
+                     "form": "the same scheduler, shortest remaining work first, per-job "
+                             "kernels"},
             "scheduler": info, "data": "synthetic",
             "config": {"series": "64 seeded: N in {512,1024,2048}, T in {41,61,81} over "
                                  "+-U(60,70) deg, th U(64,384); WBP then SIRT-10 (0.5)",
@@ -855,8 +872,10 @@ def run_serve(args):
                                  sirt_iters=r["iters"], gamma=0.5))
 
             def waiter():
-                S.wait(jid)
-                finish(k, buf)
+                try:
+                    S.wait(jid)
+                finally:  # a failed job still releases its slot (and is reported)
+                    finish(k, buf)
             t = th.Thread(target=waiter)
             t.start()
             return t

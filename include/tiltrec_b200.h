@@ -365,8 +365,8 @@ tr_status tr_sched_destroy(tr_sched *s);
  * 256 B, exceed it are rejected with TR_ERR_BUDGET, and ntilt is at most 360;
  * non-finite coefficients give TR_ERR_ARG.  The geometry is passed to the
  * device as kernel arguments, so nothing on the host is read after the call
- * returns.  The first call on a device looks up the array's device address;
- * make it before any stream capture.  Calls share the array: each clears what
+ * returns.  The first call on a device also looks up the array's device
+ * address (a synchronous runtime call).  Calls share the array: each clears what
  * must start at zero, and calls whose work overlaps on the GPU race.  A
  * back-projection whose bounded staging wait gives up leaves its volume
  * unchanged and sets a sticky report word in the array that later calls do

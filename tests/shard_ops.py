@@ -65,9 +65,12 @@ class OracleOps:
                                                              vol.numpy(), gamma)))
 
 
-def run_rank(rank, world, port, cases, out_dir, use_gpu=False):
+def run_rank(rank, world, port, cases, out_dir, use_gpu=False, backend="gloo"):
     """One rank: runs every case through autom2_b200.shard and writes the
-    gathered volume of each to out_dir/<case>_<rank>.npy."""
+    gathered volume of each to out_dir/<case>_<rank>.npy.  backend "nccl"
+    (one rank per GPU): the collectives run over NCCL on the CUDA tensors
+    themselves (shard.TorchComm); with gloo on a GPU they are staged through
+    host memory (HostStagedComm), so ranks can share one GPU."""
     import sys
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path.insert(0, root)
@@ -75,14 +78,16 @@ def run_rank(rank, world, port, cases, out_dir, use_gpu=False):
 
     from autom2_b200 import shard
 
-    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+    if backend == "nccl":
+        torch.cuda.set_device(rank)
+    dist.init_process_group(backend, init_method=f"tcp://127.0.0.1:{port}", rank=rank,
                             world_size=world,
                             timeout=__import__("datetime").timedelta(seconds=120))
     try:
         if use_gpu:
             from autom2_b200.tiltrec import Engine
-            ops = Engine(0)
-            comm = HostStagedComm()
+            ops = Engine(rank if backend == "nccl" else 0)
+            comm = shard.TorchComm() if backend == "nccl" else HostStagedComm()
             dev = "cuda"
         else:
             ops = OracleOps()

@@ -23,3 +23,21 @@ def test_two_ranks_on_the_gpu_match_whole_volume(engine, restatement, tmp_path):
             got = np.load(tmp_path / f"{name}_{rank}.npy")
             err = O.rel_l2(got, want)
             assert err < 1e-5, (name, rank, err)
+
+
+def test_nccl_rank_runs_the_collective_path(engine, restatement, tmp_path):
+    """The NCCL path of shard.TorchComm (all-reduce of the forward projections
+    and the weights on CUDA tensors, all-gather of the slabs) on the one GPU
+    this test has: a single rank, with z-slabs forced so every collective
+    runs.  Several ranks need one GPU each (NCCL refuses two ranks on one
+    device); the two-rank logic is covered on one GPU through gloo above."""
+    R = restatement
+    cases = {k: v for k, v in _cases(R).items()
+             if k in ("forced_zslabs_SIRT_0", "tilted_SIRT_1", "tilted_WBP_0")}
+    for c in cases.values():
+        c["mode"] = "zslabs"
+    run_ranks(cases, tmp_path, world=1, use_gpu=True, backend="nccl")
+    for name, c in cases.items():
+        got = np.load(tmp_path / f"{name}_0.npy")
+        assert (tmp_path / f"{name}_0.mode").read_text() == "zslabs"
+        assert O.rel_l2(got, _whole(R, c)) < 1e-5, name

@@ -99,9 +99,10 @@ def free_port():
         return s.getsockname()[1]
 
 
-def run_ranks(cases, tmp_path, world=2, use_gpu=False):
+def run_ranks(cases, tmp_path, world=2, use_gpu=False, backend="gloo"):
     from shard_ops import run_rank
-    mp.start_processes(run_rank, args=(world, free_port(), cases, str(tmp_path), use_gpu),
+    mp.start_processes(run_rank,
+                       args=(world, free_port(), cases, str(tmp_path), use_gpu, backend),
                        nprocs=world, start_method="spawn", join=True)
 
 
