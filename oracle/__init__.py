@@ -44,6 +44,13 @@ def build(with_reference: bool | None = None) -> None:
                        cwd=HERE, check=True)
 
 
+def reference_resample_executable() -> str | None:
+    """The reference's resample tool (``make ref``: its unmodified sources
+    with the test-only OpenCV subset), or None where it was not built."""
+    path = os.path.join(REF_DIR, "resample")
+    return path if os.path.exists(path) else None
+
+
 def reference_gpu_executable(layout: int = 0) -> str | None:
     """The reference's own TiltRec-cuda / TiltRecZ-cuda compiled for sm_100a
     (``make refgpu``), or None where they were not built."""

@@ -224,3 +224,46 @@ def test_resample_bin_restatement(restatement):
         g = restatement.resample_bin(b, f)
         assert g.shape == (1, 13 // f, 17 // f)
         assert abs(g.mean() - b.astype(np.float64).mean()) < 1e-6
+
+
+@pytest.mark.parametrize("shape,factor", [((2, 36, 48), 3), ((3, 37, 50), 3), ((1, 64, 40), 4)])
+@pytest.mark.parametrize("mode", [2, 1, 0])
+def test_resample_restatement_vs_reference_tool(restatement, tmp_path, shape, factor, mode):
+    """The reference's own resample tool (its unmodified sources with the
+    test-only OpenCV subset, oracle/_ref/resample) against the restatement:
+    sections read as float (bytes unsigned / 255, shorts as values), area
+    binning, a float output whose header is the input's with the new sizes
+    and mode 2 (the tool's closing statistics rewrite never reaches the file,
+    so amin / amax / amean stay the input's)."""
+    import subprocess
+    import sys
+    sys.path.insert(0, HERE)
+    from mrc_util import read_mrc, write_mrc
+    exe = O.reference_resample_executable()
+    if exe is None:
+        pytest.skip("oracle/_ref/resample is not built here")
+    rng = np.random.default_rng(sum(shape) + mode)
+    if mode == 2:
+        data = rng.normal(size=shape).astype(np.float32)
+    elif mode == 1:
+        data = np.round(rng.normal(size=shape) * 300).astype(np.float32)
+    else:
+        data = rng.integers(0, 256, size=shape).astype(np.float32)
+    src, out = tmp_path / "in.mrc", tmp_path / "out.mrc"
+    write_mrc(src, data.astype(np.uint8).view(np.int8) if mode == 0 else data, mode=mode,
+              next_bytes=32 if mode == 1 else 0)
+    with open(src, "r+b") as f:
+        f.seek(76)
+        f.write(np.array([-1.5, 2.5, 0.25], "<f4").tobytes())
+    r = subprocess.run([exe, "-i", str(src), "-o", str(out), "-b", str(factor)],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    hi, _, _ = read_mrc(src)
+    ho, _, got = read_mrc(out)
+    want = restatement.resample_bin(data / 255.0 if mode == 0 else data, factor)
+    assert got.shape == want.shape
+    assert np.abs(got - want).max() <= 1e-6 * max(1.0, np.abs(want).max())
+    assert int(ho["mode"]) == 2
+    assert [int(v) for v in ho["m"]] == [want.shape[2], want.shape[1], want.shape[0]]
+    for f in ("amin", "amax", "amean", "next"):
+        assert np.array_equal(ho[f], hi[f]), f
