@@ -714,8 +714,11 @@ __device__ __forceinline__ void mbar_init_pair(unsigned long long *mbar) {
   __syncthreads();
 }
 
+// 16-bit images: three CTAs per SM (80 registers) hold the compensated sums
+// without spilling (FP16-storage SIRT iteration on cfg1: 31.7 -> 30.5 ms);
+// FP32 images: four.
 template <int MODE, bool SEP, typename IT>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, std::is_same<IT, float>::value ? 4 : 3)
     bp_tma_kernel(const BpArgs a, const __grid_constant__ CUtensorMap tmap) {
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) unsigned long long mbar[2];
@@ -1228,7 +1231,8 @@ __global__ void __launch_bounds__(kThreads, 4) fp_batch_kernel(BatchTable *T) {
 // Back-projection items: BP_NORM over FP32 images (filtered projections) and
 // BP_SIRT over residuals of type RT.
 template <typename RT>
-__global__ void __launch_bounds__(kThreads, 4) bp_batch_kernel(BatchTable *T) {
+__global__ void __launch_bounds__(kThreads, std::is_same<RT, float>::value ? 4 : 3)
+    bp_batch_kernel(BatchTable *T) {
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ __align__(8) unsigned long long mbar[2];
   __shared__ long long s_tile;
