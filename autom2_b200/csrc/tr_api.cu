@@ -1186,6 +1186,79 @@ namespace {
 
 // Uploads the host stack (and the starting volume, or zeroes it) to the
 // context's device copies and runs `method` on them, ordered on io_stream.
+// Host memory the GPU can copy asynchronously (page-locked or registered).
+bool host_pinned(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Copies sections [z0, z0 + nz) of the device volume into the host volume.
+cudaError_t vol_sections_d2h(const tr_ctx *c, float *host, const float *dev, int z0, int nz,
+                             cudaStream_t s) {
+  const size_t nx = c->nx, ny = c->ny;
+  if (c->layout == TR_LAYOUT_Z)
+    return cudaMemcpyAsync(host + (size_t)z0 * nx * ny, dev + (size_t)z0 * nx * ny,
+                           (size_t)nz * nx * ny * sizeof(float), cudaMemcpyDeviceToHost, s);
+  const size_t pitch = nx * (size_t)c->th * sizeof(float);
+  return cudaMemcpy2DAsync(host + (size_t)z0 * nx, pitch, dev + (size_t)z0 * nx, pitch,
+                           (size_t)nz * nx * sizeof(float), ny, cudaMemcpyDeviceToHost, s);
+}
+
+// SIRT from page-locked host buffers with the copies overlapped: the stack's
+// upload runs on a copy stream while the geometry-only weights are computed,
+// and the last iteration's update runs in z-slabs (about four, tile-aligned)
+// whose sections go back to the host while the next slab updates.  The same
+// launches as tr_sirt, so the same volume.
+tr_status sirt_host_overlapped(tr_ctx *c, const float *proj_h, float *vol_h, bool zero_start,
+                               int iters, float gamma) {
+  const size_t pn = proj_elems(c), vn = vol_elems(c);
+  tr_status st = host_buffers(c);
+  if (st || (st = slab_streams(c))) return st;
+  cudaStream_t s = c->io_stream;
+  TR_CUDA(c, cudaEventRecord(c->ev_start, s));
+  TR_CUDA(c, cudaStreamWaitEvent(c->cp_in, c->ev_start, 0));
+  TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, pn * sizeof(float), cudaMemcpyHostToDevice,
+                             c->cp_in));
+  if (!zero_start)
+    TR_CUDA(c, cudaMemcpyAsync(c->hvol_d, vol_h, vn * sizeof(float), cudaMemcpyHostToDevice,
+                               c->cp_in));
+  TR_CUDA(c, cudaEventRecord(c->ev_in[0], c->cp_in));
+  if (zero_start) TR_CUDA(c, cudaMemsetAsync(c->hvol_d, 0, vn * sizeof(float), s));
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection")) ||
+      (st = ensure_wt(c, s)) || (st = ensure_wtvol(c, 0, c->th, s)))
+    return st;
+  TR_CUDA(c, cudaStreamWaitEvent(s, c->ev_in[0], 0));
+  if (iters > 1 && (st = tr_sirt(c, c->hproj_d, c->hvol_d, iters - 1, gamma, s))) return st;
+  if (iters > 0) {  // the last iteration: forward projection and residual as tr_sirt
+    TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
+    TR_CUDA(c, launch_fp(c->sep, fp_args(c, c->hvol_d, 0, c->th, c->val_d, 0, c->nt), s));
+    TR_CUDA(c, launch_resid(c->hproj_d, c->val_d, c->wt_d, pn, c->nsm, s));
+  }
+  const int depth = c->th >= 4 * kTZ ? slab_depth(c, c->th / 4) : c->th;
+  const dim3 g = bp_tile_grid(full_view(c, nullptr, 0, c->th));
+  int k = 0;
+  for (int z0 = 0; z0 < c->th; z0 += depth, k = (k + 1) % kSlabBufs) {
+    const int nz = std::min(depth, c->th - z0);
+    if (iters > 0) {
+      BpArgs b = bp_args(c, nullptr, z0, nz, c->val_d, 0, c->nt, gamma);
+      b.v = slab_view(c, c->hvol_d, false, z0, nz);
+      set_weights(c, &b);
+      b.wslot = c->wslot_d + (size_t)(z0 / kTZ) * g.x * g.y;  // this slab's tiles
+      TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
+    }
+    TR_CUDA(c, cudaEventRecord(c->ev_comp[k], s));
+    TR_CUDA(c, cudaStreamWaitEvent(c->cp_out, c->ev_comp[k], 0));
+    TR_CUDA(c, vol_sections_d2h(c, vol_h, c->hvol_d, z0, nz, c->cp_out));
+  }
+  TR_CUDA(c, cudaStreamSynchronize(c->cp_out));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  return take_timeout(c);
+}
+
 tr_status run_host_method(tr_ctx *c, int method, const float *proj_h, const float *vol_h,
                           bool zero_start, int iters, float gamma) {
   const size_t pn = proj_elems(c), vn = vol_elems(c);
@@ -1219,6 +1292,9 @@ tr_status tr_reconstruct_host(tr_ctx *c, int method, const float *proj_h, float 
   if (st) return st;
   if (!proj_h || !vol_h) return fail(c, TR_ERR_ARG, "null host buffer");
   const bool zero_start = (method & TR_RECON_ZERO_START) != 0;
+  if ((method & ~TR_RECON_ZERO_START) == TR_METHOD_SIRT && iters >= 0 && host_pinned(proj_h) &&
+      host_pinned(vol_h))
+    return sirt_host_overlapped(c, proj_h, vol_h, zero_start, iters, gamma);
   if ((st = run_host_method(c, method & ~TR_RECON_ZERO_START, proj_h, vol_h, zero_start, iters,
                             gamma)))
     return st;

@@ -398,3 +398,39 @@ def test_bounded_wait_gives_up(engine, golden):
     engine.wbp(dev(g("proj")), vol)
     engine.synchronize()
     assert O.rel_l2(host(vol), g("wbp")) < TOL
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("th,zero_start,iters", [(160, True, 3), (160, False, 2), (40, True, 2),
+                                                  (130, False, 1), (128, True, 0)])
+def test_host_sirt_with_overlapped_copies(engine, restatement, layout, th, zero_start, iters):
+    """tr_reconstruct_host SIRT from page-locked buffers: the stack uploads
+    while the weights are computed and the last update runs in z-slabs whose
+    sections copy back while the next slab updates.  Same volume as the
+    device path (1e-6: the forward projection's float atomic order) and the
+    oracle."""
+    R = restatement
+    rng = np.random.default_rng(th + layout + iters)
+    nx, ny, nt = 64, 24, 9
+    ang = np.linspace(-60, 60, nt).astype(np.float32)
+    c8 = R.coeffs(ang, 0.5, 1.5, 0.0)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    vshape = (ny, th, nx) if layout == 0 else (th, ny, nx)
+    vol0 = (np.zeros(vshape, np.float32) if zero_start
+            else rng.normal(size=vshape).astype(np.float32) * 0.1)
+    org = T.default_origin(layout, nx, ny, th)
+    engine.set_problem(nx, ny, nt, th, c8, layout, org)
+    want = dev(vol0)
+    engine.sirt(dev(proj), want, iters, 0.5)
+    ph = torch.from_numpy(proj).pin_memory()
+    vh = torch.from_numpy(np.full(vshape, np.nan, np.float32) if zero_start else vol0.copy())
+    vh = vh.pin_memory()
+    engine.reconstruct_host("SIRT", ph.numpy(), vh.numpy(), iters, 0.5, zero_start=zero_start)
+    got = vh.numpy()
+    assert np.isfinite(got).all()
+    if iters == 0:  # the starting volume comes back unchanged
+        assert np.array_equal(got, host(want))
+        return
+    assert O.rel_l2(got, host(want)) < 1e-6
+    g = R.geom(nx, ny, nt, th, layout, 0, org)
+    assert O.rel_l2(got, R.sirt(g, c8, proj, vol0, iters, 0.5)) < 1e-5
