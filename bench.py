@@ -53,8 +53,10 @@ def peaks():
 # by component to the full launch: voxel-side bytes x 8, detector-side bytes
 # x 4.  fp_kernel: 134.2 MB volume read x 8 + (66.7 MB read + 67.4 MB
 # written) x 4; bp_tma_kernel (SIRT): (134.2 MB volume read + 110.3 MB
-# written) x 8 + 240.4 MB detector-side reads x 4.  The captures and their
-# commands are summarised in profiles/fp_kernel.md and profiles/bp_kernel.md.
+# written) x 8 + 240.4 MB detector-side reads x 4.  Captured with
+#   ncu --set full --clock-control none -k regex:<kernel> -s <n> -c 1 \
+#       python bench.py --kernels --scale 2 --iters 2
+# (fp_kernel: -s 4, the first timed iteration's; bp_tma_kernel: -s 1).
 TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": 1.6100e9, "bp_kernel": 2.9173e9}
 
 
