@@ -121,8 +121,9 @@ struct tr_sched {
   std::thread worker;
   std::string err;
   tr_status fatal = TR_OK;
-  // TR_SCHED_BATCHED or TR_SCHED_SRPT
+  // TR_SCHED_BATCHED or TR_SCHED_SRPT, and the SRPT aging time (0: none)
   int policy = TR_SCHED_BATCHED;
+  double aging_s = 0;
   // counters
   long long steps = 0, items_bp = 0, items_fp = 0;
 };
@@ -445,15 +446,23 @@ double job_work(const Job &j) {
   return ((j.wbp_pending ? 1.0 : 0.0) + 2.0 * j.iters_left) * j.d.ntilt * (double)j.nvox;
 }
 
+// SRPT order key: the work left, divided by 1 + (time since submission) /
+// aging time, so that a long job's priority grows while it waits.
+double srpt_key(const tr_sched *S, const Job &j, double now) {
+  const double w = job_work(j);
+  return S->aging_s > 0 ? w / (1.0 + (now - j.t_submit) / S->aging_s) : w;
+}
+
 // TR_SCHED_SRPT step: the next unit of the ready job with the least remaining
 // work (its WBP back-projection, or one SIRT iteration) through the per-job
 // kernels the context path runs.  At most two steps are in flight, so a job
 // that becomes ready is considered within one step.
 tr_status launch_job_step(tr_sched *S, bool *launched) {
   Job *j = nullptr;
+  const double now = now_s();
   for (auto &jp : S->active)
     if (jp->state == J_READY && (jp->wbp_pending || jp->iters_left > 0) &&
-        (!j || job_work(*jp) < job_work(*j)))
+        (!j || srpt_key(S, *jp, now) < srpt_key(S, *j, now)))
       j = jp.get();
   if (!j) return TR_OK;
   const int b = S->next_tab;
@@ -607,11 +616,12 @@ tr_status progress(tr_sched *S, bool *busy) {
   // Admit while a job fits: the queue's head in order (TR_SCHED_BATCHED), or
   // the queued job with the least work that fits (TR_SCHED_SRPT).  With
   // nothing admitted, the chosen job is admitted whatever its size.
+  const double now = now_s();
   while (!S->queue.empty()) {
     auto pick = S->queue.begin();
     if (S->policy == TR_SCHED_SRPT)
       for (auto it = S->queue.begin(); it != S->queue.end(); ++it)
-        if (job_work(**it) < job_work(**pick) &&
+        if (srpt_key(S, **it, now) < srpt_key(S, **pick, now) &&
             (!S->budget || S->used + (*it)->bytes <= S->budget))
           pick = it;
     Job &j = **pick;
@@ -828,6 +838,13 @@ tr_status tr_sched_set_policy(tr_sched *S, int policy) {
   if (!S || (policy != TR_SCHED_BATCHED && policy != TR_SCHED_SRPT)) return TR_ERR_ARG;
   std::lock_guard<std::mutex> lk(S->mu);
   S->policy = policy;
+  return TR_OK;
+}
+
+tr_status tr_sched_set_aging(tr_sched *S, double aging_s) {
+  if (!S || !(aging_s >= 0)) return TR_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->aging_s = aging_s;
   return TR_OK;
 }
 

@@ -443,6 +443,7 @@ class Scheduler:
         L.tr_sched_last_error.restype = C.c_char_p
         L.tr_sched_configure.argtypes = [vp, sz, i]
         L.tr_sched_set_policy.argtypes = [vp, i]
+        L.tr_sched_set_aging.argtypes = [vp, C.c_double]
         L.tr_sched_autotune.argtypes = [vp, C.POINTER(Job), i, C.POINTER(sz), C.POINTER(i)]
         L.tr_sched_destroy.argtypes = [vp]
         h = vp()
@@ -508,6 +509,10 @@ class Scheduler:
         kernels)."""
         self._check(self.lib.tr_sched_set_policy(self.h, {"batched": 0, "srpt": 1}[policy]),
                     "tr_sched_set_policy")
+
+    def set_aging(self, aging_s: float):
+        """SRPT aging time in seconds (0: pure shortest remaining work)."""
+        self._check(self.lib.tr_sched_set_aging(self.h, aging_s), "tr_sched_set_aging")
 
     def autotune(self, probe: Job, iters: int = 2):
         sm, ct = C.c_size_t(), C.c_int()

@@ -764,7 +764,9 @@ def run_serve(args):
         tr_reconstruct_host (FP32), a FIFO single server;
       * the scheduler (16-bit storage) under each step policy, fed by a
         front end that keeps --inflight requests submitted (the shortest
-        pending one next under SRPT, the oldest under the batched policy).
+        pending one next under SRPT, the oldest under the batched policy):
+        pure shortest remaining work, the same aged (work divided by
+        1 + wait / --aging, in the front end and the scheduler), batched.
     Latency runs from arrival to the volume in host memory.  Each request's
     middle volume row from the scheduler is compared with the plain FP32
     result (relative L2)."""
@@ -834,7 +836,13 @@ def run_serve(args):
                     if state["next"] < n:
                         wait = min(wait, max(0.0, reqs[state["next"]]["t"] - now))
                     lock.wait(timeout=wait)
-                k = min(pending, key=work) if order == "srpt" else pending[0]
+                if order == "fifo" or order == "batched":
+                    k = pending[0]
+                else:  # shortest work first, aged for "srpt_aged"
+                    age = args.aging if order == "srpt_aged" else 0.0
+                    now = time.perf_counter() - start
+                    k = min(pending, key=lambda q: work(q) / (
+                        1.0 + (now - reqs[q]["t"]) / age if age > 0 else 1.0))
                 pending.remove(k)
                 state["inflight"] += 1
                 buf = free[series[reqs[k]["cls"]][0].nx].pop()
@@ -862,9 +870,11 @@ def run_serve(args):
     free_b, _ = torch.cuda.mem_get_info()
     budget = min(int(args.budget_gb * 1e9), int(free_b - 8e9))
     forms = {}
-    for policy in ("srpt", "batched"):
+    for form in ("srpt", "srpt_aged", "batched"):
         S = T.Scheduler(0, hbm_budget=budget, proj_dtype=args.storage, resid_dtype=args.storage)
-        S.set_policy(policy)
+        S.set_policy("batched" if form == "batched" else "srpt")
+        if form == "srpt_aged":
+            S.set_aging(args.aging)
 
         def sched_one(k, buf, finish, S=S):
             r = reqs[k]
@@ -882,11 +892,11 @@ def run_serve(args):
             t.start()
             return t
 
-        lat, span, rows = serve(sched_one, policy, K)
+        lat, span, rows = serve(sched_one, form, K)
         info = S.stats()
         S.close()
         errs = [oracle_free_rel_l2(a, b) for a, b in zip(rows, rows_p)]
-        forms[policy] = {"value": n / span * 3600, "makespan_s": span,
+        forms[form] = {"value": n / span * 3600, "makespan_s": span,
                          "p50_latency_s": pct(lat, 50), "p99_latency_s": pct(lat, 99),
                          "mean_latency_s": float(np.mean(lat)),
                          "rel_l2_vs_plain_f32_middle_row": {"max": max(errs),
@@ -946,6 +956,8 @@ def main():
                     help="serve: arrivals per second (default 4)")
     ap.add_argument("--inflight", type=int, default=4,
                     help="serve: requests the front end keeps submitted")
+    ap.add_argument("--aging", type=float, default=5.0,
+                    help="serve: aging time (s) of the aged shortest-work-first form")
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--storage", default="f16", choices=["f32", "f16", "bf16"])
     args = ap.parse_args()

@@ -288,7 +288,8 @@ tr_status tr_autotune_zslab(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
  *  - TR_SCHED_SRPT: shortest remaining work first.  Admission takes the
  *    queued job with the least work that fits; each step runs the next unit
  *    (WBP back-projection or SIRT iteration) of the ready job with the least
- *    work left, through the same per-job kernels as tr_sirt / tr_wbp.
+ *    work left, through the same per-job kernels as tr_sirt / tr_wbp
+ *    (optionally aged: tr_sched_set_aging).
  * A background thread drives the steps; calls are thread-safe.
  * Results do not depend on the other jobs in the mix beyond the order of the
  * forward projection's float atomic adds (as for a job run alone).  Images
@@ -340,6 +341,11 @@ tr_status tr_sched_configure(tr_sched *s, size_t smem_bp, int bp_ctas_per_sm);
 /* Step policy (TR_SCHED_BATCHED / TR_SCHED_SRPT); takes effect at the next
  * step or admission. */
 tr_status tr_sched_set_policy(tr_sched *s, int policy);
+/* TR_SCHED_SRPT aging: a job's remaining work counts divided by
+ * 1 + (seconds since submission) / aging_s when jobs are ordered, so that a
+ * long job's priority grows while it waits (bounding its delay behind a
+ * stream of short ones).  0 (the default): pure shortest remaining work. */
+tr_status tr_sched_set_aging(tr_sched *s, double aging_s);
 /* Autotuner: times `iters` SIRT steps of a device-resident probe job (run on
  * a scratch copy of its volume) under candidate configurations -- shared
  * memory per back-projection CTA (40, 56, 80, 112 KiB) at full residency,

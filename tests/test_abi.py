@@ -64,6 +64,13 @@ def test_errors_without_device_or_problem(lib):
     assert lib.tr_geometry_from_angles(None, 3, 0, 0, 0, None) == -1
     assert lib.tr_set_problem(None, 8, 8, 1, 4, 0, None, 0, 0, 0) == -1
     assert lib.tr_sirt(None, None, None, 1, 0.5, None) == -1
+    lib.tr_sched_set_aging.argtypes = [C.c_void_p, C.c_double]
+    assert lib.tr_sched_set_aging(None, 1.0) == -1
+    assert lib.tr_sched_set_policy(None, 1) == -1
+    lib.tr_sirt_zslabs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
+                                   C.c_void_p]
+    assert lib.tr_sirt_zslabs(None, None, 0, None, 0, None, 0, 1, 0.5, 32, None) == -1
 
 
 def test_engine_fails_loudly_without_gpu():

@@ -166,7 +166,7 @@ def test_autotune_picks_a_candidate(engine, restatement):
         S.close()
 
 
-@pytest.mark.parametrize("policy", ["batched", "srpt"])
+@pytest.mark.parametrize("policy", ["batched", "srpt", "srpt_aged"])
 def test_jobs_admitted_while_another_is_mid_iteration(engine, restatement, policy):
     """Continuous batching: a long SIRT job is already stepping when two more
     jobs arrive; they are admitted while it runs, run alongside it (batched)
@@ -185,7 +185,9 @@ def test_jobs_admitted_while_another_is_mid_iteration(engine, restatement, polic
                          proj=rng.normal(size=(nt, ny, nx)).astype(np.float32),
                          wbp=k == 2, iters=iters, gamma=0.5))
     S = T.Scheduler(0)
-    S.set_policy(policy)
+    S.set_policy("srpt" if policy.startswith("srpt") else policy)
+    if policy == "srpt_aged":  # aged, but the long job's wait stays short of overtaking
+        S.set_aging(600.0)
     try:
         keep, ids, t_sub = [], [], []
 
