@@ -728,6 +728,12 @@ def run_batch(args):
     S.set_policy("srpt")
     t_srpt, lat_srpt, errs_srpt = run_sched()
     S.close()
+    # The same policy with FP32 storage (the plain form's): the scheduler's own
+    # cost, without the 16-bit conversions.
+    S = T.Scheduler(0, hbm_budget=budget, proj_dtype="f32", resid_dtype="f32")
+    S.set_policy("srpt")
+    t_srpt32, lat_srpt32, errs_srpt32 = run_sched()
+    S.close()
     line = {"workload": "batch", "metric": "voxel-proj updates/s", "unit": "VPU/s",
             "value": total_vpu / t_batch, "n_gpus": 1, "higher_is_better": True,
             "jobs": len(series), "recon_per_hour": len(series) / t_batch * 3600,
@@ -747,6 +753,11 @@ def run_batch(args):
                      "rel_l2_vs_plain_f32_max": max(errs_srpt),
                      "form": "the same scheduler, shortest remaining work first, per-job "
                              "kernels"},
+            "srpt_f32_storage": {"value": total_vpu / t_srpt32, "seconds": t_srpt32,
+                                 "recon_per_hour": len(series) / t_srpt32 * 3600,
+                                 "speedup_vs_plain": t_plain / t_srpt32,
+                                 "p50_latency_s": statistics.median(lat_srpt32),
+                                 "rel_l2_vs_plain_f32_max": max(errs_srpt32)},
             "scheduler": info, "data": "synthetic",
             "config": {"series": "64 seeded: N in {512,1024,2048}, T in {41,61,81} over "
                                  "+-U(60,70) deg, th U(64,384); WBP then SIRT-10 (0.5)",
