@@ -85,6 +85,11 @@ struct tr_ctx {
   // z-slab SIRT: the next iteration's reprojection, the device staging slabs
   // of a host-resident volume, their copy streams and events
   float *val2_d = nullptr, *slab_d = nullptr;
+  // deterministic forward projections (tr_set_deterministic): int64 sums
+  // [ntilt][ny][nx] and the view's max |voxel|
+  bool deterministic = false;
+  unsigned long long *ival_d = nullptr;
+  unsigned *gmax_d = nullptr;
   cudaStream_t cp_in = nullptr, cp_out = nullptr;
   cudaEvent_t ev_in[3] = {}, ev_comp[3] = {}, ev_free[3] = {}, ev_start = nullptr;
 };
@@ -106,6 +111,13 @@ tr_status fail(tr_ctx *c, tr_status s, const char *fmt, ...) {
 tr_status cuda_fail(tr_ctx *c, cudaError_t e, const char *what) {
   return fail(c, TR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
+
+// Returns the tr_status of `call` when it is not TR_OK.
+#define TR_TRY(call)                \
+  do {                              \
+    const tr_status s_ = (call);    \
+    if (s_ != TR_OK) return s_;     \
+  } while (0)
 
 #define TR_CUDA(ctx, call)                                  \
   do {                                                      \
@@ -244,7 +256,7 @@ tr_status take_timeout(tr_ctx *c) {
 
 FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
                int t0, int nt) {
-  FpArgs a;
+  FpArgs a{};
   a.v = full_view(c, const_cast<float *>(vol), z0, nz);
   a.val = val;
   a.tstride = (long long)c->nx * c->ny;
@@ -261,6 +273,24 @@ FpArgs fp_args(const tr_ctx *c, const float *vol, int z0, int nz, float *val,
   a.chunk = c->chunk_fp;
   a.nbound = c->fp_nbound;
   return a;
+}
+
+// A forward projection through the context: the float flush, or with
+// tr_set_deterministic the int64 one (sums cleared first, converted after).
+tr_status run_fp(tr_ctx *c, const FpArgs &a, cudaStream_t s) {
+  if (!c->deterministic) {
+    TR_CUDA(c, launch_fp(c->sep, a, s));
+    return TR_OK;
+  }
+  tr_status st;
+  if ((st = scratch_alloc(c, (void **)&c->ival_d, proj_elems(c) * sizeof(unsigned long long),
+                          "deterministic projection sums")) ||
+      (st = scratch_alloc(c, (void **)&c->gmax_d, sizeof(unsigned), "largest voxel")))
+    return st;
+  const size_t off = (size_t)a.t0 * a.tstride, n = (size_t)a.nt * a.tstride;
+  TR_CUDA(c, cudaMemsetAsync(c->ival_d + off, 0, n * sizeof(unsigned long long), s));
+  TR_CUDA(c, launch_fp_deterministic(c->sep, a, c->ival_d, c->gmax_d, c->nsm, s));
+  return TR_OK;
 }
 
 // Kernel spectrum of the R-weighting filter for rows of nx samples.
@@ -366,7 +396,7 @@ tr_status ensure_wt(tr_ctx *c, cudaStream_t s) {
   if (!c->wt_ready) {
     TR_CUDA(c, cudaMemsetAsync(c->wt_d, 0, pb, s));
     FpArgs a = fp_args(c, nullptr, 0, c->th, c->wt_d, 0, c->nt);
-    TR_CUDA(c, launch_fp(c->sep, a, s));
+    if ((st = run_fp(c, a, s))) return st;
     c->wt_ready = true;
   }
   return TR_OK;
@@ -584,7 +614,7 @@ tr_status slab_sweep(tr_ctx *c, const SlabRun &r, int zend, const void *res, con
     if (fp_out) {
       FpArgs f = fp_args(c, nullptr, z0, nz, fp_out, 0, c->nt);
       f.v = v;
-      TR_CUDA(c, launch_fp(c->sep, f, s));
+      TR_TRY(run_fp(c, f, s));
     }
     if (r.host) {
       if (write_back) {
@@ -828,10 +858,10 @@ tr_status tr_forward_project(tr_ctx *c, const float *vol, int z0, int nz, float 
   if (!vol || !val || z0 < 0 || nz < 1 || z0 + nz > c->th)
     return fail(c, TR_ERR_ARG, "bad forward-projection arguments (z0=%d nz=%d)", z0, nz);
   FpArgs a = fp_args(c, vol, z0, nz, val, 0, c->nt);
-  TR_CUDA(c, launch_fp(c->sep, a, (cudaStream_t)stream));
+  TR_TRY(run_fp(c, a, (cudaStream_t)stream));
   if (wt) {
     FpArgs w = fp_args(c, nullptr, z0, nz, wt, 0, c->nt);
-    TR_CUDA(c, launch_fp(c->sep, w, (cudaStream_t)stream));
+    TR_TRY(run_fp(c, w, (cudaStream_t)stream));
   }
   return TR_OK;
 }
@@ -846,11 +876,11 @@ tr_status tr_forward_project_tilts(tr_ctx *c, const float *vol, int z0, int nz, 
                 z0, nz, t0, ntilts);
   FpArgs a = fp_args(c, vol, z0, nz, val, 0, ntilts);
   a.geo = c->geo_d + t0;
-  TR_CUDA(c, launch_fp(c->sep, a, (cudaStream_t)stream));
+  TR_TRY(run_fp(c, a, (cudaStream_t)stream));
   if (wt) {
     FpArgs w = fp_args(c, nullptr, z0, nz, wt, 0, ntilts);
     w.geo = c->geo_d + t0;
-    TR_CUDA(c, launch_fp(c->sep, w, (cudaStream_t)stream));
+    TR_TRY(run_fp(c, w, (cudaStream_t)stream));
   }
   return TR_OK;
 }
@@ -907,7 +937,7 @@ tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gam
   for (int it = 0; it < iters; ++it) {
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
     FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
-    TR_CUDA(c, launch_fp(c->sep, f, s));
+    TR_TRY(run_fp(c, f, s));
     TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
     BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, 0, c->nt, gamma);
     set_weights(c, &b);
@@ -932,7 +962,7 @@ tr_status tr_sart(tr_ctx *c, const float *proj, float *vol, int iters, float gam
       float *vt = c->val_d + plane * t;
       TR_CUDA(c, cudaMemsetAsync(vt, 0, plane * sizeof(float), s));
       FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, t, 1);
-      TR_CUDA(c, launch_fp(c->sep, f, s));
+      TR_TRY(run_fp(c, f, s));
       TR_CUDA(c, launch_resid(proj + plane * t, vt, c->wt_d + plane * t, plane, c->nsm, s));
       BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, t, 1, gamma);
       TR_CUDA(c, run_bp(c, BP_NORM, b, s));
@@ -1000,7 +1030,7 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
   for (int it = 0; it < iters; ++it) {
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
     FpArgs f = fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt);
-    TR_CUDA(c, launch_fp(c->sep, f, s));
+    TR_TRY(run_fp(c, f, s));
     if (rdtype == TR_DTYPE_F16) {
       // The residual's range is not the stack's (a WBP start, for one, makes
       // it larger): form it in FP32, then store it with its own per-tilt
@@ -1019,6 +1049,13 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
     set_weights(c, &b);
     TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
+  return TR_OK;
+}
+
+tr_status tr_set_deterministic(tr_ctx *c, int on) {
+  if (!c) return TR_ERR_ARG;
+  c->deterministic = on != 0;
+  c->wt_ready = false;  // recompute the projection weights the same way
   return TR_OK;
 }
 
@@ -1127,7 +1164,7 @@ tr_status tr_admm(tr_ctx *c, const float *proj, float *vol, int outer, int cg_it
   auto apply = [&](const float *x, float *out) -> tr_status {
     TR_CUDA(c, cudaMemsetAsync(out, 0, V * sizeof(float), s));
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
-    TR_CUDA(c, launch_fp(c->sep, fp_args(c, x, 0, c->th, c->val_d, 0, c->nt), s));
+    TR_TRY(run_fp(c, fp_args(c, x, 0, c->th, c->val_d, 0, c->nt), s));
     TR_CUDA(c, admm_normalize(c->val_d, c->wt_d, pn, nsm, s));
     TR_CUDA(c, run_bp(c, BP_SUM, bp_args(c, out, 0, c->th, c->val_d, 0, c->nt, 1.f), s));
     TR_CUDA(c, admm_add_scaled(out, x, mu, V, nsm, s));
@@ -1235,7 +1272,7 @@ tr_status sirt_host_overlapped(tr_ctx *c, const float *proj_h, float *vol_h, boo
   if (iters > 1 && (st = tr_sirt(c, c->hproj_d, c->hvol_d, iters - 1, gamma, s))) return st;
   if (iters > 0) {  // the last iteration: forward projection and residual as tr_sirt
     TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
-    TR_CUDA(c, launch_fp(c->sep, fp_args(c, c->hvol_d, 0, c->th, c->val_d, 0, c->nt), s));
+    TR_TRY(run_fp(c, fp_args(c, c->hvol_d, 0, c->th, c->val_d, 0, c->nt), s));
     TR_CUDA(c, launch_resid(c->hproj_d, c->val_d, c->wt_d, pn, c->nsm, s));
   }
   const int depth = c->th >= 4 * kTZ ? slab_depth(c, c->th / 4) : c->th;

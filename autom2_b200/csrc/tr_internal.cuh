@@ -106,6 +106,14 @@ struct FpArgs {
   float ox, oy, oz;
   int fw, fh, chunk;
   float nbound;       // most voxel contributions one window entry can collect
+  // Deterministic flush (ival != nullptr): each pixel accumulates int64 fixed
+  // point at the launch-wide scale fp_gscale(gmax, gbound), so integer adds in
+  // any order give the same sums; launch_ival_to_val then adds them into val.
+  // gmax: the view's largest |voxel| as float bits (nullptr: ones, 1);
+  // gbound: the view's voxel count, which bounds any pixel's sum / max|v|.
+  unsigned long long *ival;
+  const unsigned *gmax;
+  double gbound;
 };
 
 // Footprint bookkeeping of one tilt for one tile, computed in FP64.
@@ -227,6 +235,11 @@ cudaError_t launch_classify_tiles(const TiltGeo *geo, int nt, const VolView &v, 
 cudaError_t launch_sep_row_weights(const TiltGeo *geo, int nt, int ny, float oy, int pny,
                                    float *wrow, cudaStream_t s);
 cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s);
+// Deterministic forward projection into a.val: the view's max |voxel| into
+// *gmax, the splat with the int64 flush into ival (all zero on entry, left
+// zero), then the sums converted and added into a.val.
+cudaError_t launch_fp_deterministic(bool sep, FpArgs a, unsigned long long *ival,
+                                    unsigned *gmax, int nsm, cudaStream_t s);
 cudaError_t launch_resid(const float *p, float *val, const float *wt, size_t n, int nsm,
                          cudaStream_t s);
 cudaError_t launch_quantize(const float *p, size_t plane, int nt, int dtype, void *out,

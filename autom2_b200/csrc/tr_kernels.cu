@@ -757,6 +757,18 @@ __device__ __forceinline__ void red_add_v4(float *p, float x, float y, float z, 
                : "memory");
 }
 
+// Launch-wide fixed-point scale of the deterministic flush: the largest power
+// of two S with S * gbound * max|v| <= 2^62, so no pixel's int64 sum can
+// overflow (each voxel adds at most |v| to a pixel in total); 0 when the view
+// is all zero.
+__device__ __forceinline__ double fp_gscale(const unsigned *gmax, double gbound) {
+  const float vmax = gmax ? __uint_as_float(*gmax) : 1.f;
+  if (!(vmax > 0.f)) return 0.0;
+  int e;
+  frexp(4.611686018427387904e18 / (gbound * (double)vmax), &e);
+  return ldexp(1.0, e - 1);
+}
+
 // A forward-projection CTA's shared bookkeeping.  Declared once per kernel and
 // passed in, so that a kernel instantiating both fp_tile forms holds one copy.
 struct FpShared {
@@ -835,6 +847,7 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
   }
   int *const iacc = reinterpret_cast<int *>(accs);
   const bool s_scale_nonzero = s_nonzero != 0;  // an all-zero tile adds nothing
+  const double gS = a.ival ? fp_gscale(a.gmax, a.gbound) : 0.0;
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
@@ -932,6 +945,8 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       const int kmin = tt[i].kmin, nq = tt[i].nq, nr = tt[i].nr;
       const int *T = iacc + (size_t)i * per;
       float *base = a.val + (size_t)(a.t0 + c0 + i) * a.tstride;
+      unsigned long long *ibase =
+          a.ival ? a.ival + (size_t)(a.t0 + c0 + i) * a.tstride : nullptr;
       const float inv = s_inv;
       const int ngq = (nq + 3) >> 2;
       for (int e = tid; e < nr * ngq; e += kThreads) {
@@ -944,6 +959,15 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
         const bool inside = vec_ok && k >= 0 && k + 3 < a.pnx;
         auto add_row = [&](int j, float wgt) {
           if ((unsigned)j >= (unsigned)a.pny) return;
+          if (ibase) {  // deterministic: int64 adds at the launch-wide scale
+            unsigned long long *ip = ibase + (size_t)j * a.pnx + k;
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+              if (s[m] != 0.f && (unsigned)(k + m) < (unsigned)a.pnx)
+                atomicAdd(ip + m,
+                          (unsigned long long)__double2ll_rn((double)(s[m] * wgt) * gS));
+            return;
+          }
           float *p = base + (size_t)j * a.pnx + k;
           if (inside && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
             red_add_v4(p, s[0] * wgt, s[1] * wgt, s[2] * wgt, s[3] * wgt);
@@ -1516,6 +1540,59 @@ cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     fp_kernel<false><<<fp_grid(a.v), kThreads, smem, s>>>(a);
   }
+  return cudaGetLastError();
+}
+
+// Largest |voxel| of a view, as float bits, max-combined into *out (which
+// starts at 0).  Walks x fastest, then the view's smaller-stride axis.
+__global__ void absmax_view_kernel(const VolView v, unsigned *out) {
+  const size_t n = (size_t)v.nx * v.ny * v.nz;
+  const bool zy = v.sz < v.sy;  // [y][z][x] (Y layout): z before y
+  unsigned m = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % v.nx);
+    const size_t r = i / v.nx;
+    const int a = zy ? (int)(r % v.nz) : (int)(r % v.ny);
+    const int b = zy ? (int)(r / v.nz) : (int)(r / v.ny);
+    const int z = zy ? a : b, y = zy ? b : a;
+    m = max(m, __float_as_uint(fabsf(v.vol[(size_t)y * v.sy + (size_t)z * v.sz + x])));
+  }
+  m = __reduce_max_sync(0xffffffffu, m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
+// Adds the deterministic flush's int64 sums into val and clears them.
+__global__ void ival_to_val_kernel(unsigned long long *ival, float *val, size_t n,
+                                   const unsigned *gmax, double gbound) {
+  const double S = fp_gscale(gmax, gbound);
+  const double inv = S > 0.0 ? 1.0 / S : 0.0;  // S is a power of two
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const long long q = (long long)ival[i];
+    if (q) {
+      val[i] += (float)((double)q * inv);
+      ival[i] = 0ull;
+    }
+  }
+}
+
+cudaError_t launch_fp_deterministic(bool sep, FpArgs a, unsigned long long *ival,
+                                    unsigned *gmax, int nsm, cudaStream_t s) {
+  a.ival = ival;
+  a.gbound = (double)a.v.nx * a.v.ny * a.v.nz;
+  a.gmax = nullptr;
+  cudaError_t e;
+  if (a.v.vol) {
+    if ((e = cudaMemsetAsync(gmax, 0, sizeof(unsigned), s)) != cudaSuccess) return e;
+    absmax_view_kernel<<<nsm * 4, 256, 0, s>>>(a.v, gmax);
+    a.gmax = gmax;
+  }
+  if ((e = launch_fp(sep, a, s)) != cudaSuccess) return e;
+  const size_t n = (size_t)a.nt * a.tstride, off = (size_t)a.t0 * a.tstride;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
+  ival_to_val_kernel<<<blocks > 0 ? blocks : 1, 256, 0, s>>>(ival + off, a.val + off, n, a.gmax,
+                                                            a.gbound);
   return cudaGetLastError();
 }
 

@@ -158,7 +158,7 @@ tr_status run(int device, int nx, int ny, int nt, int th, int layout,
   v.sy = layout == TR_LAYOUT_Y ? (long long)th * nx : nx;
   v.sz = layout == TR_LAYOUT_Y ? nx : (long long)ny * nx;
 
-  FpArgs f;
+  FpArgs f{};
   f.v = v;
   f.tstride = (long long)nx * ny;
   f.pnx = nx;

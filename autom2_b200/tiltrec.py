@@ -106,6 +106,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_backproject_lp.argtypes = [vp, vp, i, vp, vp, i, i, vp]
     lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
     lib.tr_sirt_zslabs.argtypes = [vp, vp, i, vp, i, vp, i, i, f, i, vp]
+    lib.tr_set_deterministic.argtypes = [vp, i]
     lib.tr_autotune_zslab.argtypes = [vp, vp, i, vp, i, vp, i, C.POINTER(i), dp]
     lib.tr_synchronize.argtypes = [vp]
     lib.tr_selftest_wait.argtypes = [vp, i]
@@ -341,6 +342,12 @@ class Engine:
                                                _ptr(scale), DTYPES[resid_dtype], vp, host,
                                                C.byref(d), C.byref(ms)), "tr_autotune_zslab")
         return d.value, ms.value
+
+    def set_deterministic(self, on: bool = True):
+        """tr_set_deterministic: int64 fixed-point forward-projection sums,
+        bitwise repeatable."""
+        self._check(self.lib.tr_set_deterministic(self.h, int(bool(on))),
+                    "tr_set_deterministic")
 
     def synchronize(self):
         self._check(self.lib.tr_synchronize(self.h), "tr_synchronize")

@@ -258,6 +258,19 @@ tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
  * forward projection's float atomic adds.  Device memory: two reprojections
  * (ntilt*ny*nx floats each), the weights, and with a host volume three slabs
  * of depth*ny*nx floats. */
+/* Deterministic forward projections for this context (on != 0; off by
+ * default).  The splat's window flush then adds each pixel's contributions
+ * as int64 fixed point at one launch-wide scale (the largest power of two S
+ * with S * voxels * max|v| <= 2^62, so no sum can overflow; each contribution
+ * rounded from the same float value the default flush adds), and the sums are
+ * converted and added into the output afterwards.  Integer addition is
+ * associative, so tr_forward_project and every SIRT / SART / ADMM / z-slab
+ * call of the context give bitwise-identical results run to run (the
+ * back-projection is deterministic in both modes).  Costs a reduction over
+ * the volume, int64 sums of twice the stack's bytes and a conversion pass per
+ * forward projection.  Scheduler and tr_sirt_static calls are not affected. */
+tr_status tr_set_deterministic(tr_ctx *ctx, int on);
+
 tr_status tr_sirt_zslabs(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
                          const float *scale_dev, int resid_dtype, float *vol,
                          int vol_on_host, int iters, float gamma, int depth,

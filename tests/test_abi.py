@@ -67,6 +67,8 @@ def test_errors_without_device_or_problem(lib):
     lib.tr_sched_set_aging.argtypes = [C.c_void_p, C.c_double]
     assert lib.tr_sched_set_aging(None, 1.0) == -1
     assert lib.tr_sched_set_policy(None, 1) == -1
+    lib.tr_set_deterministic.argtypes = [C.c_void_p, C.c_int]
+    assert lib.tr_set_deterministic(None, 1) == -1
     lib.tr_sirt_zslabs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
                                    C.c_void_p]

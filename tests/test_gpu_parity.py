@@ -434,3 +434,45 @@ def test_host_sirt_with_overlapped_copies(engine, restatement, layout, th, zero_
     assert O.rel_l2(got, host(want)) < 1e-6
     g = R.geom(nx, ny, nt, th, layout, 0, org)
     assert O.rel_l2(got, R.sirt(g, c8, proj, vol0, iters, 0.5)) < 1e-5
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("name", ["xtilt", "rotated", "sep_big_shift"])
+def test_deterministic_forward_projection(engine, restatement, name, layout):
+    """tr_set_deterministic: the forward projection's flush adds int64 fixed
+    point at one launch-wide scale, so repeated SIRT runs are bitwise equal;
+    the sums match the default float flush (1e-6) and the oracle (1e-5), also
+    with one voxel 1e4 times the rest (the scale follows the largest voxel, so
+    the others keep float-like precision)."""
+    R = restatement
+    nx, ny, nt, th, c8, proj, vol0, org = _random_case(R, name, layout)
+    g = R.geom(nx, ny, nt, th, layout, 0, org)
+    engine.set_problem(nx, ny, nt, th, c8, layout, org)
+    try:
+        default = dev(vol0)
+        engine.sirt(dev(proj), default, 3, 0.5)
+        engine.set_deterministic(True)
+        runs = []
+        for _ in range(2):
+            v = dev(vol0)
+            engine.sirt(dev(proj), v, 3, 0.5)
+            runs.append(host(v))
+        assert np.array_equal(runs[0], runs[1])
+        assert O.rel_l2(runs[0], host(default)) < 1e-6
+        assert O.rel_l2(runs[0], R.sirt(g, c8, proj, vol0, 3, 0.5)) < 1e-5
+        spiky = vol0.copy()
+        spiky.reshape(-1)[spiky.size // 3] = 1e4 * np.abs(vol0).max()
+        val = torch.zeros((nt, ny, nx), device="cuda")
+        engine.forward_project(dev(spiky), val)
+        got = host(val)
+        for t in range(nt):
+            want, _ = R.reproject(g, c8[t], spiky)
+            base, _ = R.reproject(g, c8[t], vol0)
+            assert O.rel_l2(got[t], want) < TOL, t
+            # away from the spike's footprint, the ordinary values keep their
+            # precision under the spike-sized scale
+            away = want == base
+            scale = np.abs(base).max()
+            assert np.abs(got[t][away] - want[away]).max() <= 1e-5 * scale, t
+    finally:
+        engine.set_deterministic(False)
