@@ -746,8 +746,9 @@ __global__ void __launch_bounds__(kThreads, std::is_same<IT, float>::value ? 4 :
 // voxel pair's combined contribution stays within the exact range of the
 // float-shift rounding (|x| < 2^22).  Each contribution is rounded
 // to the nearest integer of its scaled value (a quantum of
-// nbound * max|v| * 2^-30, ~1e-9 of the tile's largest value for tilts
-// within +-60 degrees); the sums are exact and independent of atomic order.
+// max(nbound 2^-30, 2^-20) max|v|: with nbound <= 768 for tilts within
+// +-60 degrees, an error of at most ~5e-7 of the tile's largest |v|); the
+// sums are exact and independent of atomic order.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
 // Adds four floats to four consecutive global floats (16-byte aligned).
