@@ -946,6 +946,45 @@ tr_status tr_sirt(tr_ctx *c, const float *proj, float *vol, int iters, float gam
   return TR_OK;
 }
 
+tr_status tr_sirt_gated(tr_ctx *c, const float *proj, float *vol, int max_iters, float gamma,
+                        double rel_tol, double *norms, int *iters_done, void *stream) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj || !vol || max_iters < 0 || !(rel_tol >= 0))
+    return fail(c, TR_ERR_ARG, "bad gated SIRT arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t pn = proj_elems(c);
+  if ((st = scratch_alloc(c, (void **)&c->val_d, pn * sizeof(float), "reprojection")) ||
+      (st = scratch_alloc(c, (void **)&c->admm_dot_d, (kAdmmParts + 3) * sizeof(double),
+                          "residual norm")) ||
+      (st = ensure_wt(c, s)) || (st = ensure_wtvol(c, 0, c->th, s)))
+    return st;
+  double *part = c->admm_dot_d, *dnorm = part + kAdmmParts;
+  double prev = 0;
+  int done = 0;
+  for (int it = 0; it < max_iters; ++it) {
+    TR_CUDA(c, cudaMemsetAsync(c->val_d, 0, pn * sizeof(float), s));
+    TR_TRY(run_fp(c, fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt), s));
+    TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
+    // |r|^2 in FP64 with fixed-order partial sums, read back to gate
+    TR_CUDA(c, admm_dot(c->val_d, c->val_d, pn, part, dnorm, s));
+    double h = 0;
+    TR_CUDA(c, cudaMemcpyAsync(&h, dnorm, sizeof(double), cudaMemcpyDeviceToHost, s));
+    TR_CUDA(c, cudaStreamSynchronize(s));
+    const double nrm = sqrt(h);
+    if (norms) norms[it] = nrm;
+    if (it > 0 && rel_tol > 0 && prev - nrm < rel_tol * prev) break;  // converged
+    BpArgs b = bp_args(c, vol, 0, c->th, c->val_d, 0, c->nt, gamma);
+    set_weights(c, &b);
+    TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
+    prev = nrm;
+    done = it + 1;
+  }
+  if (iters_done) *iters_done = done;
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  return take_timeout(c);
+}
+
 tr_status tr_sart(tr_ctx *c, const float *proj, float *vol, int iters, float gamma,
                   void *stream) {
   tr_status st = need_problem(c);

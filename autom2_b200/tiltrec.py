@@ -107,6 +107,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_sirt_lp.argtypes = [vp, vp, i, vp, i, vp, i, f, vp]
     lib.tr_sirt_zslabs.argtypes = [vp, vp, i, vp, i, vp, i, i, f, i, vp]
     lib.tr_set_deterministic.argtypes = [vp, i]
+    lib.tr_sirt_gated.argtypes = [vp, vp, vp, i, f, d, vp, C.POINTER(i), vp]
     lib.tr_autotune_zslab.argtypes = [vp, vp, i, vp, i, vp, i, C.POINTER(i), dp]
     lib.tr_synchronize.argtypes = [vp]
     lib.tr_selftest_wait.argtypes = [vp, i]
@@ -342,6 +343,16 @@ class Engine:
                                                _ptr(scale), DTYPES[resid_dtype], vp, host,
                                                C.byref(d), C.byref(ms)), "tr_autotune_zslab")
         return d.value, ms.value
+
+    def sirt_gated(self, proj, vol, max_iters, gamma, rel_tol=0.0):
+        """tr_sirt_gated: (iterations applied, FP64 residual norms)."""
+        norms = np.zeros(max(1, max_iters), np.float64)
+        done = C.c_int()
+        self._check(self.lib.tr_sirt_gated(self.h, _ptr(proj), _ptr(vol), max_iters, gamma,
+                                           rel_tol, norms.ctypes.data, C.byref(done),
+                                           _stream(self.device)), "tr_sirt_gated")
+        n = min(max_iters, done.value + 1) if max_iters else 0
+        return done.value, norms[:n]
 
     def set_deterministic(self, on: bool = True):
         """tr_set_deterministic: int64 fixed-point forward-projection sums,

@@ -152,6 +152,17 @@ tr_status tr_sirt(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
 
 /* SART, in place.  SART (main-mpi.cpp:578-612; main-mpiz.cpp:502-546),
  * CuSART / CuSARTZ (recon_y.cuh:35, recon_z.cuh:26). */
+/* SIRT (as tr_sirt) with an FP64 convergence gate.  Each iteration's
+ * residual r = p - val/wt has its L2 norm summed in FP64 on the device
+ * (fixed-order partial sums, so the norms repeat exactly) and read back; the
+ * iterations stop before applying an update once the norm fell by less than
+ * rel_tol of the previous one (rel_tol 0: run all max_iters).  norms_out
+ * (host, max_iters doubles, may be NULL) receives every residual norm
+ * computed, including the one that stopped the loop; *iters_done the updates
+ * applied.  Blocking. */
+tr_status tr_sirt_gated(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
+                        int max_iters, float gamma, double rel_tol,
+                        double *norms_out, int *iters_done, void *stream);
 tr_status tr_sart(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
                   int iters, float gamma, void *stream);
 

@@ -69,6 +69,9 @@ def test_errors_without_device_or_problem(lib):
     assert lib.tr_sched_set_policy(None, 1) == -1
     lib.tr_set_deterministic.argtypes = [C.c_void_p, C.c_int]
     assert lib.tr_set_deterministic(None, 1) == -1
+    lib.tr_sirt_gated.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_float, C.c_double,
+                                                   C.c_void_p, C.c_void_p, C.c_void_p]
+    assert lib.tr_sirt_gated(None, None, None, 3, 0.5, 0.0, None, None, None) == -1
     lib.tr_sirt_zslabs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
                                    C.c_void_p]

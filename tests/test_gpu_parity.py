@@ -478,3 +478,34 @@ def test_deterministic_forward_projection(engine, restatement, name, layout):
         assert O.rel_l2(got, flt) < 1e-6
     finally:
         engine.set_deterministic(False)
+
+
+def test_sirt_gated_fp64_norms(engine, restatement):
+    """tr_sirt_gated: the residual norms are FP64 sums of the FP32 residual
+    (the first, from a zero volume, is exactly |p| in FP64), decrease, repeat
+    exactly, and a relative tolerance stops the loop before an update; with
+    no tolerance the volume is tr_sirt's."""
+    R = restatement
+    nx, ny, nt, th, c8, proj, vol0, org = _random_case(R, "xtilt", 1)
+    engine.set_problem(nx, ny, nt, th, c8, 1, org)
+    p = dev(proj)
+    zero = np.zeros_like(vol0)
+    v = dev(zero)
+    done, norms = engine.sirt_gated(p, v, 6, 0.5)
+    assert done == 6 and len(norms) == 6
+    assert abs(norms[0] - np.linalg.norm(proj.astype(np.float64))) <= 1e-12 * norms[0]
+    assert np.all(np.diff(norms) < 0)
+    w = dev(zero)
+    engine.sirt(p, w, 6, 0.5)
+    assert O.rel_l2(host(v), host(w)) < 1e-6
+    _, again = engine.sirt_gated(p, dev(zero), 6, 0.5)
+    assert O.rel_l2(again, norms) < 1e-6
+    # stop once an iteration removes less than 30 % of the residual norm
+    v = dev(zero)
+    done, nr = engine.sirt_gated(p, v, 20, 0.5, rel_tol=0.3)
+    assert 0 < done < 20 and len(nr) == done + 1
+    assert nr[-2] - nr[-1] < 0.3 * nr[-2]
+    assert all(nr[k - 1] - nr[k] >= 0.3 * nr[k - 1] for k in range(1, done))
+    w = dev(zero)
+    engine.sirt(p, w, done, 0.5)
+    assert O.rel_l2(host(v), host(w)) < 1e-6
