@@ -53,14 +53,16 @@ __global__ void admm_cg_init_kernel(float *r, float *p, const float *__restrict_
 }
 
 // sum of the float products a[i]*b[i] in FP64 (the reference multiplies in
-// float and accumulates in double, :886-891, :916): per-block partials.
+// float and accumulates in double, :886-891, :916), or with PROD64 the exact
+// FP64 products: per-block partials.
+template <bool PROD64>
 __global__ void admm_dot_partial_kernel(const float *__restrict__ a, const float *__restrict__ b,
                                         size_t n, double *part) {
   __shared__ double red[256];
   double s = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    s += (double)(a[i] * b[i]);
+    s += PROD64 ? (double)a[i] * (double)b[i] : (double)(a[i] * b[i]);
   red[threadIdx.x] = s;
   __syncthreads();
   for (int o = blockDim.x / 2; o; o >>= 1) {
@@ -159,7 +161,14 @@ cudaError_t admm_cg_init(float *r, float *p, const float *b, const float *a, siz
 // Deterministic FP64 dot product into *out; part holds kAdmmParts doubles.
 cudaError_t admm_dot(const float *a, const float *b, size_t n, double *part, double *out,
                      cudaStream_t s) {
-  admm_dot_partial_kernel<<<kAdmmParts, 256, 0, s>>>(a, b, n, part);
+  admm_dot_partial_kernel<false><<<kAdmmParts, 256, 0, s>>>(a, b, n, part);
+  admm_dot_finish_kernel<<<1, 256, 0, s>>>(part, kAdmmParts, out);
+  return cudaGetLastError();
+}
+
+// |a|^2 with FP64 products and fixed-order FP64 sums into *out.
+cudaError_t sumsq_f64(const float *a, size_t n, double *part, double *out, cudaStream_t s) {
+  admm_dot_partial_kernel<true><<<kAdmmParts, 256, 0, s>>>(a, a, n, part);
   admm_dot_finish_kernel<<<1, 256, 0, s>>>(part, kAdmmParts, out);
   return cudaGetLastError();
 }

@@ -967,7 +967,7 @@ tr_status tr_sirt_gated(tr_ctx *c, const float *proj, float *vol, int max_iters,
     TR_TRY(run_fp(c, fp_args(c, vol, 0, c->th, c->val_d, 0, c->nt), s));
     TR_CUDA(c, launch_resid(proj, c->val_d, c->wt_d, pn, c->nsm, s));
     // |r|^2 in FP64 with fixed-order partial sums, read back to gate
-    TR_CUDA(c, admm_dot(c->val_d, c->val_d, pn, part, dnorm, s));
+    TR_CUDA(c, sumsq_f64(c->val_d, pn, part, dnorm, s));
     double h = 0;
     TR_CUDA(c, cudaMemcpyAsync(&h, dnorm, sizeof(double), cudaMemcpyDeviceToHost, s));
     TR_CUDA(c, cudaStreamSynchronize(s));

@@ -263,6 +263,8 @@ cudaError_t admm_atb(float *atb, const float *u, const float *d, float mu, size_
                      cudaStream_t s);
 cudaError_t admm_cg_init(float *r, float *p, const float *b, const float *a, size_t n, int nsm,
                          cudaStream_t s);
+// |a|^2 with FP64 products and fixed-order FP64 sums (kAdmmParts partials).
+cudaError_t sumsq_f64(const float *a, size_t n, double *part, double *out, cudaStream_t s);
 cudaError_t admm_dot(const float *a, const float *b, size_t n, double *part, double *out,
                      cudaStream_t s);
 cudaError_t admm_x_update(float *vol, const float *p, const double *scal, size_t n, int nsm,
