@@ -742,13 +742,13 @@ __global__ void __launch_bounds__(kThreads, std::is_same<IT, float>::value ? 4 :
 // tile's values are scaled by a power of two S chosen from the tile's largest
 // |voxel| so that no window entry can overflow: an entry collects at most
 // `nbound` voxel contributions (host bound from the x slope) of magnitude at
-// most max|v|, and S <= 2^30 / (nbound max|v|); also S <= 2^20 / max|v| so a
-// voxel pair's combined contribution stays within the exact range of the
-// float-shift rounding (|x| < 2^22).  Each contribution is rounded
-// to the nearest integer of its scaled value (a quantum of
-// max(nbound 2^-30, 2^-20) max|v|: with nbound <= 768 for tilts within
-// +-60 degrees, an error of at most ~5e-7 of the tile's largest |v|); the
-// sums are exact and independent of atomic order.
+// most max|v|, and S <= 2^30 / (nbound max|v|); also S <= 2^21 / max|v| so
+// every scaled contribution stays within the exact range of the float-shift
+// rounding (|x| < 2^22).  Each contribution is rounded to the nearest integer
+// of its scaled value (a quantum of max(nbound 2^-30, 2^-21) max|v|: with
+// nbound <= 768 for tilts within +-60 degrees, an error of at most ~5e-7 of
+// the tile's largest |v|, ~2.5e-7 where |a1| > 2/3); the sums are exact and
+// independent of atomic order.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
 // Adds four floats to four consecutive global floats (16-byte aligned).
@@ -830,7 +830,7 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       unsigned mm = 0;
       for (int w = 0; w < kThreads / 32; ++w) mm = max(mm, wmax[w]);
       const float vmax = __uint_as_float(mm);
-      float lim = vmax > 0.f ? fminf(1073741824.0f / (a.nbound * vmax), 1048576.0f / vmax)
+      float lim = vmax > 0.f ? fminf(1073741824.0f / (a.nbound * vmax), 2097152.0f / vmax)
                              : 1.f;
       int ex;
       frexpf(lim, &ex);  // lim = m 2^ex, m in [0.5, 1): 2^(ex-1) <= lim
