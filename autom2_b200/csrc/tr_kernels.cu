@@ -781,7 +781,7 @@ struct FpShared {
   int nonzero;
 };
 
-template <bool SEP>
+template <bool SEP, bool DET = false>
 __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
                                         float *accs, FpShared &sh) {
   TileTilt *const tt = sh.tt;
@@ -848,7 +848,9 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
   }
   int *const iacc = reinterpret_cast<int *>(accs);
   const bool s_scale_nonzero = s_nonzero != 0;  // an all-zero tile adds nothing
-  const double gS = a.ival ? fp_gscale(a.gmax, a.gbound) : 0.0;
+  // DET: the deterministic int64 flush (a.ival), a separate instantiation so
+  // that the default flush carries none of it.
+  const double gS = DET ? fp_gscale(a.gmax, a.gbound) : 0.0;
 
   for (int c0 = 0; c0 < a.nt; c0 += a.chunk) {
     const int nc = min(a.chunk, a.nt - c0);
@@ -947,7 +949,7 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       const int *T = iacc + (size_t)i * per;
       float *base = a.val + (size_t)(a.t0 + c0 + i) * a.tstride;
       unsigned long long *ibase =
-          a.ival ? a.ival + (size_t)(a.t0 + c0 + i) * a.tstride : nullptr;
+          DET ? a.ival + (size_t)(a.t0 + c0 + i) * a.tstride : nullptr;
       const float inv = s_inv;
       const int ngq = (nq + 3) >> 2;
       for (int e = tid; e < nr * ngq; e += kThreads) {
@@ -960,7 +962,7 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
         const bool inside = vec_ok && k >= 0 && k + 3 < a.pnx;
         auto add_row = [&](int j, float wgt) {
           if ((unsigned)j >= (unsigned)a.pny) return;
-          if (ibase) {  // deterministic: int64 adds at the launch-wide scale
+          if (DET) {  // deterministic: int64 adds at the launch-wide scale
             unsigned long long *ip = ibase + (size_t)j * a.pnx + k;
 #pragma unroll
             for (int m = 0; m < 4; ++m)
@@ -992,11 +994,11 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
   }
 }
 
-template <bool SEP>
-__global__ void __launch_bounds__(kThreads, SEP ? 3 : 4) fp_kernel(const FpArgs a) {
+template <bool SEP, bool DET>
+__global__ void __launch_bounds__(kThreads, SEP || DET ? 3 : 4) fp_kernel(const FpArgs a) {
   extern __shared__ __align__(16) float accs[];
   __shared__ FpShared sh;
-  fp_tile<SEP>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs, sh);
+  fp_tile<SEP, DET>(a, blockIdx.x, blockIdx.y, blockIdx.z, accs, sh);
 }
 
 // SIRT residual (main/main-mpi.cpp:640-647): r = p - (wt != 0 ? val/wt : val),
@@ -1526,22 +1528,21 @@ static dim3 fp_grid(const VolView &v) {
               (v.nz + kFTZ - 1) / kFTZ);
 }
 
+template <bool SEP, bool DET>
+static cudaError_t launch_fp_t(const FpArgs &a, size_t smem, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(fp_kernel<SEP, DET>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fp_kernel<SEP, DET><<<fp_grid(a.v), kThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fp(bool sep, const FpArgs &a, cudaStream_t s) {
   const int fh = sep ? kTY : a.fh;
   const size_t smem = (size_t)a.chunk * fh * a.fw * sizeof(float);
-  cudaError_t e;
-  if (sep) {
-    e = cudaFuncSetAttribute(fp_kernel<true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    fp_kernel<true><<<fp_grid(a.v), kThreads, smem, s>>>(a);
-  } else {
-    e = cudaFuncSetAttribute(fp_kernel<false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    fp_kernel<false><<<fp_grid(a.v), kThreads, smem, s>>>(a);
-  }
-  return cudaGetLastError();
+  if (a.ival)
+    return sep ? launch_fp_t<true, true>(a, smem, s) : launch_fp_t<false, true>(a, smem, s);
+  return sep ? launch_fp_t<true, false>(a, smem, s) : launch_fp_t<false, false>(a, smem, s);
 }
 
 // Largest |voxel| of a view, as float bits, max-combined into *out (which
