@@ -328,7 +328,10 @@ int run(const Options &o) {
   tr_ctx *ctx = nullptr;
   int device = 0;
   if (const char *d = getenv("TILTREC_DEVICE")) device = atoi(d);
-  if (tr_create(device, 0, &ctx) != TR_OK)
+  // TILTREC_HBM_BUDGET: device-memory budget of the context in bytes (0: none)
+  size_t budget = 0;
+  if (const char *b = getenv("TILTREC_HBM_BUDGET")) budget = strtoull(b, nullptr, 10);
+  if (tr_create(device, budget, &ctx) != TR_OK)
     return fprintf(stderr, "%s: no CUDA device %d\n", kProg, device), 1;
   int st = tr_set_problem(ctx, nx, ny, nt, th, zlayout ? TR_LAYOUT_Z : TR_LAYOUT_Y, coeff.data(),
                           ox, oy, oz);
@@ -344,20 +347,22 @@ int run(const Options &o) {
   const size_t slab = zlayout ? nvox : (size_t)nx * th * 64;
   const float alpha = zlayout ? 0.f : 0.9f;
   bool ok = true;
+  // A whole volume in host memory to the output file (float, or bytes).
+  auto write_host = [&](const float *v) {
+    if (o.f2b) {
+      std::vector<float> copy(v, v + nvox);
+      std::vector<unsigned char> b = to_bytes(copy, slab, alpha);
+      std::vector<float> sec(plane);
+      for (size_t i = 0; i < plane; ++i) sec[i] = (float)b[mid * plane + i];
+      trcli::update_stats(&out, sec.data(), plane);
+      return trcli::write_volume(o.output, out, b.data(), b.size(), &err);
+    }
+    trcli::update_stats(&out, v + mid * plane, plane);
+    return trcli::write_volume(o.output, out, v, nvox * sizeof(float), &err);
+  };
   if (st == TR_OK && method == kMethodAdmm) {
     st = tr_admm_host(ctx, proj.data(), vol.data(), o.iteration, o.cgiter, o.gamma, o.soft);
-    if (st == TR_OK) {
-      if (o.f2b) {
-        std::vector<unsigned char> b = to_bytes(vol, slab, alpha);
-        std::vector<float> sec(plane);
-        for (size_t i = 0; i < plane; ++i) sec[i] = (float)b[mid * plane + i];
-        trcli::update_stats(&out, sec.data(), plane);
-        ok = trcli::write_volume(o.output, out, b.data(), b.size(), &err);
-      } else {
-        trcli::update_stats(&out, vol.data() + mid * plane, plane);
-        ok = trcli::write_volume(o.output, out, vol.data(), vol.size() * sizeof(float), &err);
-      }
-    }
+    if (st == TR_OK) ok = write_host(vol.data());
   } else if (st == TR_OK) {
     FileSink k;
     k.f = fopen(o.output.c_str(), "wb");
@@ -380,6 +385,27 @@ int run(const Options &o) {
     }
     ok = (fclose(k.f) == 0) && ok;
     if (!ok) err = "write failed for " + o.output;
+    if ((st == TR_ERR_OOM || st == TR_ERR_BUDGET) && method == TR_METHOD_SIRT) {
+      // The volume does not fit the device (or its budget): keep it in host
+      // memory and stream it through the device in z-slabs, as TiltRecZ
+      // streams through managed memory (recon_z.cu:96-100).
+      fprintf(stderr, "%s: the volume does not fit the device budget (%s); streaming it "
+              "in z-slabs from host memory\n", kProg, tr_last_error(ctx));
+      void *hv = nullptr;
+      st = tr_host_alloc(nvox * sizeof(float), &hv);
+      if (st == TR_OK) {
+        float *v = static_cast<float *>(hv);
+        if (use_initial) memcpy(v, vol.data(), nvox * sizeof(float));
+        int depth = 0;
+        st = tr_sirt_host_zslabs(ctx, proj.data(), v, !use_initial, o.iteration, o.gamma, 0,
+                                 &depth);
+        if (st == TR_OK) {
+          printf("%s: z-slab depth %d\n", kProg, depth);
+          ok = write_host(v);
+        }
+        tr_host_free(hv);
+      }
+    }
   }
   if (st != TR_OK) {
     fprintf(stderr, "%s: %s\n", kProg, tr_last_error(ctx));

@@ -72,7 +72,6 @@ struct tr_ctx {
   int filt_nx = 0, filt_npad = 0, filt_log2m = 0;
   float2 *ghat_d = nullptr, *tw_d = nullptr;
   float *hproj_d = nullptr, *hvol_d = nullptr;
-  size_t hproj_n = 0, hvol_n = 0;
   // byte output: slab partial sums and statistics, the bytes themselves
   double *f2b_part_d = nullptr;
   float *f2b_stats_d = nullptr;
@@ -360,25 +359,15 @@ tr_status load_geometry(tr_ctx *c, const double *coeff8, cudaStream_t s) {
   return TR_OK;
 }
 
-// Device copies of the host-buffer calls' stack and volume, kept across calls
-// and grown when a problem needs more.
-tr_status host_buffers(tr_ctx *c) {
-  const size_t pn = proj_elems(c), vn = vol_elems(c);
-  if (c->hproj_n < pn) {
-    if (c->hproj_d) cudaFree(c->hproj_d);
-    c->hproj_d = nullptr;
-    c->hproj_n = 0;
-    TR_CUDA(c, cudaMalloc(&c->hproj_d, pn * sizeof(float)));
-    c->hproj_n = pn;
-  }
-  if (c->hvol_n < vn) {
-    if (c->hvol_d) cudaFree(c->hvol_d);
-    c->hvol_d = nullptr;
-    c->hvol_n = 0;
-    TR_CUDA(c, cudaMalloc(&c->hvol_d, vn * sizeof(float)));
-    c->hvol_n = vn;
-  }
-  return TR_OK;
+// Device copies of the host-buffer calls' stack and (with_vol) volume:
+// scratch like the rest, kept across calls and counted against the budget.
+tr_status host_buffers(tr_ctx *c, bool with_vol = true) {
+  tr_status st = scratch_alloc(c, (void **)&c->hproj_d, proj_elems(c) * sizeof(float),
+                               "device copy of the stack");
+  if (!st && with_vol)
+    st = scratch_alloc(c, (void **)&c->hvol_d, vol_elems(c) * sizeof(float),
+                       "device copy of the volume");
+  return st;
 }
 
 tr_status need_problem(tr_ctx *c) {
@@ -742,8 +731,6 @@ tr_status tr_destroy(tr_ctx *c) {
   cudaDeviceSynchronize();
   release_problem(c);
   for (auto &kv : c->slots) scratch_free(c, kv.first);
-  if (c->hproj_d) cudaFree(c->hproj_d);
-  if (c->hvol_d) cudaFree(c->hvol_d);
   for (int i = 0; i < 2; ++i) {
     if (c->stage_h[i]) cudaFreeHost(c->stage_h[i]);
     if (c->stage_ev[i]) cudaEventDestroy(c->stage_ev[i]);
@@ -1089,6 +1076,46 @@ tr_status tr_sirt_lp(tr_ctx *c, const void *proj, int pdtype, const float *scale
     TR_CUDA(c, run_bp(c, BP_SIRT, b, s));
   }
   return TR_OK;
+}
+
+tr_status tr_host_alloc(size_t bytes, void **out) {
+  if (!out) return TR_ERR_ARG;
+  *out = nullptr;
+  if (cudaHostAlloc(out, std::max<size_t>(bytes, 1), cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return TR_ERR_OOM;
+  }
+  return TR_OK;
+}
+
+tr_status tr_host_free(void *p) {
+  if (p && cudaFreeHost(p) != cudaSuccess) {
+    cudaGetLastError();
+    return TR_ERR_CUDA;
+  }
+  return TR_OK;
+}
+
+tr_status tr_sirt_host_zslabs(tr_ctx *c, const float *proj_h, float *vol_h, int zero_start,
+                              int iters, float gamma, int depth, int *depth_used) {
+  tr_status st = need_problem(c);
+  if (st) return st;
+  if (!proj_h || !vol_h || iters < 0 || depth < 0)
+    return fail(c, TR_ERR_ARG, "bad host z-slab SIRT arguments");
+  scratch_free(c, (void **)&c->hvol_d);  // a device copy of the volume is what does not fit
+  if ((st = host_buffers(c, false))) return st;  // the stack only: the volume stays here
+  cudaStream_t s = c->io_stream;
+  TR_CUDA(c, cudaMemcpyAsync(c->hproj_d, proj_h, proj_elems(c) * sizeof(float),
+                             cudaMemcpyHostToDevice, s));
+  TR_CUDA(c, cudaStreamSynchronize(s));
+  if (zero_start) memset(vol_h, 0, vol_elems(c) * sizeof(float));
+  if (depth == 0 && (st = tr_autotune_zslab(c, c->hproj_d, TR_DTYPE_F32, nullptr, TR_DTYPE_F32,
+                                            vol_h, 1, &depth, nullptr)))
+    return st;
+  if (depth_used) *depth_used = slab_depth(c, depth);
+  return tr_sirt_zslabs(c, c->hproj_d, TR_DTYPE_F32, nullptr, TR_DTYPE_F32, vol_h, 1, iters,
+                        gamma, depth, s);
 }
 
 tr_status tr_set_deterministic(tr_ctx *c, int on) {

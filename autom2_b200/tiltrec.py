@@ -108,6 +108,7 @@ def load_library(path: str | None = None) -> C.CDLL:
     lib.tr_sirt_zslabs.argtypes = [vp, vp, i, vp, i, vp, i, i, f, i, vp]
     lib.tr_set_deterministic.argtypes = [vp, i]
     lib.tr_sirt_gated.argtypes = [vp, vp, vp, i, f, d, vp, C.POINTER(i), vp]
+    lib.tr_sirt_host_zslabs.argtypes = [vp, vp, vp, i, i, f, i, C.POINTER(i)]
     lib.tr_autotune_zslab.argtypes = [vp, vp, i, vp, i, vp, i, C.POINTER(i), dp]
     lib.tr_synchronize.argtypes = [vp]
     lib.tr_selftest_wait.argtypes = [vp, i]
@@ -343,6 +344,18 @@ class Engine:
                                                _ptr(scale), DTYPES[resid_dtype], vp, host,
                                                C.byref(d), C.byref(ms)), "tr_autotune_zslab")
         return d.value, ms.value
+
+    def sirt_host_zslabs(self, proj: np.ndarray, vol: np.ndarray, iters, gamma, depth=0,
+                         zero_start=True) -> int:
+        """tr_sirt_host_zslabs: SIRT with the volume kept in host memory,
+        streamed in z-slabs (depth 0: autotuned); returns the depth run."""
+        assert proj.dtype == np.float32 and proj.flags.c_contiguous
+        assert vol.dtype == np.float32 and vol.flags.c_contiguous
+        used = C.c_int()
+        self._check(self.lib.tr_sirt_host_zslabs(self.h, proj.ctypes.data, vol.ctypes.data,
+                                                 int(zero_start), iters, gamma, depth,
+                                                 C.byref(used)), "tr_sirt_host_zslabs")
+        return used.value
 
     def sirt_gated(self, proj, vol, max_iters, gamma, rel_tol=0.0):
         """tr_sirt_gated: (iterations applied, FP64 residual norms)."""

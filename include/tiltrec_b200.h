@@ -287,6 +287,22 @@ tr_status tr_sirt_zslabs(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
                          int vol_on_host, int iters, float gamma, int depth,
                          void *stream);
 
+/* SIRT over z-slabs from host buffers, the volume staying in host memory
+ * (volumes larger than the device budget: TiltRecZ's managed-memory
+ * streaming, TR/TiltRec_cuda_z/recon_z.cu:96-100).  The stack is copied to
+ * the device (counted in the budget); vol_host (page-locked for overlapped
+ * copies: tr_host_alloc) is the starting volume, or zeroed first when
+ * zero_start; depth 0 autotunes the slab depth (tr_autotune_zslab), and
+ * *depth_used (may be NULL) receives the depth run.  Blocking. */
+tr_status tr_sirt_host_zslabs(tr_ctx *ctx, const float *proj_host, float *vol_host,
+                              int zero_start, int iters, float gamma, int depth,
+                              int *depth_used);
+
+/* Page-locked host memory (cudaHostAlloc) for host-buffer calls, and its
+ * release. */
+tr_status tr_host_alloc(size_t bytes, void **out);
+tr_status tr_host_free(void *p);
+
 /* Picks the slab depth for tr_sirt_zslabs: times one full sweep (copies,
  * update with gamma 0 over a zero residual, forward projection; the volume's
  * values are unchanged) at depths 32, 64, 128, 256, 512 (those that fit the

@@ -72,6 +72,11 @@ def test_errors_without_device_or_problem(lib):
     lib.tr_sirt_gated.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_float, C.c_double,
                                                    C.c_void_p, C.c_void_p, C.c_void_p]
     assert lib.tr_sirt_gated(None, None, None, 3, 0.5, 0.0, None, None, None) == -1
+    lib.tr_sirt_host_zslabs.argtypes = [C.c_void_p] * 3 + [C.c_int, C.c_int, C.c_float,
+                                                         C.c_int, C.c_void_p]
+    assert lib.tr_sirt_host_zslabs(None, None, None, 1, 2, 0.5, 0, None) == -1
+    lib.tr_host_alloc.argtypes = [C.c_size_t, C.c_void_p]
+    assert lib.tr_host_alloc(16, None) == -1
     lib.tr_sirt_zslabs.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
                                    C.c_void_p]

@@ -311,3 +311,45 @@ def test_mpi_dialect_rejects_cuda_only_options(case):
         r = subprocess.run([exe, "--input", str(d / "stack.mrc"), *extra], capture_output=True,
                            text=True, timeout=60)
         assert r.returncode != 0, extra
+
+
+@pytest.mark.parametrize("layout", [0, 1])
+def test_volume_beyond_the_budget_streams_zslabs(tmp_path, layout):
+    """A SIRT volume that does not fit the device budget (TILTREC_HBM_BUDGET)
+    is kept in host memory and streamed through the device in autotuned
+    z-slabs, as TiltRecZ streams through managed memory: the same file as the
+    run without a budget."""
+    build.build()
+    rng = np.random.default_rng(8 + layout)
+    nx, ny, nt, th = 128, 32, 9, 256
+    ang = np.linspace(-30, 30, nt).astype(np.float32)
+    proj = rng.normal(size=(nt, ny, nx)).astype(np.float32)
+    write_mrc(tmp_path / "s.mrc", proj)
+    write_angles(tmp_path / "s.rawtlt", ang)
+    common = ["--input", str(tmp_path / "s.mrc"), "--tiltfile", str(tmp_path / "s.rawtlt"),
+              "--geometry", f"0,0,0,{th}", "--method", "SIRT,3,0.5"]
+    ours(layout, *common, "--output", str(tmp_path / "whole.mrc"))
+    # device memory of the two forms, as the library counts it
+    c8 = T.geometry_from_angles(ang)
+    org = T.default_origin(layout, nx, ny, th)
+    vshape = (ny, th, nx) if layout == 0 else (th, ny, nx)
+    e = T.Engine(0)
+    e.set_problem(nx, ny, nt, th, c8, layout, org)
+    e.reconstruct_host("SIRT", proj.copy(), np.zeros(vshape, np.float32), 3, 0.5,
+                       zero_start=True)
+    whole_bytes = e.scratch_bytes
+    e.close()
+    e = T.Engine(0)
+    e.set_problem(nx, ny, nt, th, c8, layout, org)
+    assert e.sirt_host_zslabs(proj.copy(), np.zeros(vshape, np.float32), 3, 0.5, 32) == 32
+    slab_bytes = e.scratch_bytes
+    e.close()
+    assert slab_bytes < whole_bytes
+    budget = slab_bytes + (whole_bytes - slab_bytes) // 4
+    exe = os.path.join(BIN, "TiltRec-cuda" if layout == 0 else "TiltRecZ-cuda")
+    r = subprocess.run([exe, *common, "--output", str(tmp_path / "slabs.mrc")],
+                       capture_output=True, text=True, timeout=300,
+                       env={**os.environ, "TILTREC_HBM_BUDGET": str(budget)})
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "streaming it in z-slabs" in r.stderr
+    compare(tmp_path / "slabs.mrc", tmp_path / "whole.mrc", tol=1e-6)
