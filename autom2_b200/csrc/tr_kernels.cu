@@ -46,8 +46,10 @@
 namespace trb {
 
 __device__ __forceinline__ float one_plus_frac(unsigned long long U) {
-  // 1 + (low 32 bits / 2^32), truncated to the 23-bit float mantissa.
-  return __uint_as_float(0x3F800000u | ((unsigned)U >> 9));
+  // 1 + (low 32 bits / 2^32), truncated to the 23-bit float mantissa: one
+  // funnel shift of 0x7F:low by 9 puts 0x7F << 23 = 0x3F800000 above the
+  // fraction's top 23 bits.
+  return __uint_as_float(__funnelshift_r((unsigned)U, 0x7Fu, 9));
 }
 
 // Image element -> float.
@@ -55,10 +57,37 @@ __device__ __forceinline__ float to_f(float v) { return v; }
 __device__ __forceinline__ float to_f(__half v) { return __half2float(v); }
 __device__ __forceinline__ float to_f(__nv_bfloat16 v) { return __bfloat162float(v); }
 
-// Adds the scaled contribution x (|x| <= 2^21) to a fixed-point window entry,
-// rounded to the nearest integer by the 1.5*2^23 float shift.
-__device__ __forceinline__ void wadd(int *p, float x) {
-  atomicAdd(p, __float_as_int(x + 12582912.0f) - 0x4B400000);
+// The 1.5*2^23 float shift: its bits are 0x4B400000 + round(x) for
+// |x| < 2^22, so the difference of two shifted values is the difference of
+// the rounded ones (the forward splat's fixed-point windows).
+constexpr int kFshiftBias = 0x4B400000;
+__device__ __forceinline__ int fshift(float x) { return __float_as_int(x + 12582912.0f); }
+
+// Paired FP32 arithmetic (sm_100 f32x2): two lanes of float math per
+// instruction on 64-bit register pairs {lo, hi}.
+using f32x2 = unsigned long long;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 r, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) {
@@ -744,11 +773,14 @@ __global__ void __launch_bounds__(kThreads, std::is_same<IT, float>::value ? 4 :
 // `nbound` voxel contributions (host bound from the x slope) of magnitude at
 // most max|v|, and S <= 2^30 / (nbound max|v|); also S <= 2^21 / max|v| so
 // every scaled contribution stays within the exact range of the float-shift
-// rounding (|x| < 2^22).  Each contribution is rounded to the nearest integer
-// of its scaled value (a quantum of max(nbound 2^-30, 2^-21) max|v|: with
-// nbound <= 768 for tilts within +-60 degrees, an error of at most ~5e-7 of
-// the tile's largest |v|, ~2.5e-7 where |a1| > 2/3); the sums are exact and
-// independent of atomic order.
+// rounding (|x| < 2^22).  Per voxel and window row, the row's scaled value y
+// and its upper-column part t are each rounded to the nearest integer; the
+// upper tap adds round(t) and the lower round(y) - round(t), so a tap is off
+// by at most one quantum of max(nbound 2^-30, 2^-21) max|v| (nbound <= 768
+// for tilts within +-60 degrees: ~1e-6 of the tile's largest |v|, ~5e-7
+// where |a1| > 2/3) and a row's two taps by half a quantum together; the
+// sums are exact and independent of atomic order.  The arithmetic of a
+// lane's two voxels runs side by side in f32x2 instructions.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
 // float accumulators.
 // Adds four floats to four consecutive global floats (16-byte aligned).
@@ -886,18 +918,24 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       unsigned long long UB = UA + (unsigned long long)A0;
       if (SEP) {
         int *T = iacc + (size_t)(i * kTY + wy) * fw;
+        const f32x2 one2 = pack2(1.f, 1.f), shift2 = pack2(12582912.0f, 12582912.0f);
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
-          // dx*v as one rounding of (1+dx)*v - v; the pair's lanes are two x
-          // apart, so one instruction's lanes hit distinct columns.
-          const float vA = va[k], vB = vb[k];
-          const float t1a = fmaf(one_plus_frac(UA), vA, -vA), t0a = vA - t1a;
-          const float t1b = fmaf(one_plus_frac(UB), vB, -vB), t0b = vB - t1b;
+          // The pair's voxels side by side in f32x2 arithmetic: t = v dx and
+          // v rounded once each (float shift); the lower column gets
+          // round(v) - round(t), the upper round(t).  The pair's lanes are two
+          // x apart, so one instruction's lanes hit distinct columns.
+          const f32x2 v2 = pack2(va[k], vb[k]);
+          const f32x2 fx = sub2(pack2(one_plus_frac(UA), one_plus_frac(UB)), one2);
+          float rva, rvb, rta, rtb;
+          unpack2(add2(v2, shift2), rva, rvb);
+          unpack2(add2(mul2(fx, v2), shift2), rta, rtb);
+          const int ta = __float_as_int(rta), tb = __float_as_int(rtb);
           int *ea = T + (int)(UA >> 32), *eb = T + (int)(UB >> 32);
-          wadd(ea, t0a);
-          wadd(ea + 1, t1a);
-          wadd(eb, t0b);
-          wadd(eb + 1, t1b);
+          atomicAdd(ea, __float_as_int(rva) - ta);
+          atomicAdd(ea + 1, ta - kFshiftBias);
+          atomicAdd(eb, __float_as_int(rvb) - tb);
+          atomicAdd(eb + 1, tb - kFshiftBias);
           UA += (unsigned long long)A2;
           UB += (unsigned long long)A2;
         }
@@ -906,30 +944,42 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
         unsigned long long VA = (unsigned long long)(st.Wv[warp] + (2 * lane) * B0);
         unsigned long long VB = VA + (unsigned long long)B0;
         int *T = iacc + (size_t)i * per;
+        const f32x2 one2 = pack2(1.f, 1.f), two2 = pack2(2.f, 2.f);
+        const f32x2 shift2 = pack2(12582912.0f, 12582912.0f);
 #pragma unroll
         for (int k = 0; k < kFNV; ++k) {
-          const float vA = va[k], vB = vb[k];
+          // The pair's voxels side by side in f32x2 arithmetic.  Rows:
+          // y0 = v (1 - dy) with 1 - dy = 2 - (1 + dy) exact, y1 = v - y0.
+          // Each row's pair of taps: the row's value y and its upper-column
+          // part t = y dx are rounded once each (float shift), the lower
+          // column gets round(y) - round(t), so the two taps add up to
+          // round(y) exactly.
+          const f32x2 v2 = pack2(va[k], vb[k]);
+          const f32x2 y0 = mul2(sub2(two2, pack2(one_plus_frac(VA), one_plus_frac(VB))), v2);
+          const f32x2 y1 = sub2(v2, y0);
+          const f32x2 fx = sub2(pack2(one_plus_frac(UA), one_plus_frac(UB)), one2);
+          float r0a, r0b, r01a, r01b, r1a, r1b, r11a, r11b;
+          unpack2(add2(y0, shift2), r0a, r0b);
+          unpack2(add2(mul2(fx, y0), shift2), r01a, r01b);
+          unpack2(add2(y1, shift2), r1a, r1b);
+          unpack2(add2(mul2(fx, y1), shift2), r11a, r11b);
           {
-            const float y1 = fmaf(one_plus_frac(VA), vA, -vA), y0 = vA - y1;
-            const float fx = one_plus_frac(UA);
-            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
-            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            const int r0 = __float_as_int(r0a), r01 = __float_as_int(r01a);
+            const int r1 = __float_as_int(r1a), r11 = __float_as_int(r11a);
             int *e = T + (int)(VA >> 32) * fw + (int)(UA >> 32);
-            wadd(e, t00);
-            wadd(e + 1, t01);
-            wadd(e + fw, t10);
-            wadd(e + fw + 1, t11);
+            atomicAdd(e, r0 - r01);
+            atomicAdd(e + 1, r01 - kFshiftBias);
+            atomicAdd(e + fw, r1 - r11);
+            atomicAdd(e + fw + 1, r11 - kFshiftBias);
           }
           {
-            const float y1 = fmaf(one_plus_frac(VB), vB, -vB), y0 = vB - y1;
-            const float fx = one_plus_frac(UB);
-            const float t01 = fmaf(fx, y0, -y0), t00 = y0 - t01;
-            const float t11 = fmaf(fx, y1, -y1), t10 = y1 - t11;
+            const int r0 = __float_as_int(r0b), r01 = __float_as_int(r01b);
+            const int r1 = __float_as_int(r1b), r11 = __float_as_int(r11b);
             int *e = T + (int)(VB >> 32) * fw + (int)(UB >> 32);
-            wadd(e, t00);
-            wadd(e + 1, t01);
-            wadd(e + fw, t10);
-            wadd(e + fw + 1, t11);
+            atomicAdd(e, r0 - r01);
+            atomicAdd(e + 1, r01 - kFshiftBias);
+            atomicAdd(e + fw, r1 - r11);
+            atomicAdd(e + fw + 1, r11 - kFshiftBias);
           }
           UA += (unsigned long long)A2;
           UB += (unsigned long long)A2;
