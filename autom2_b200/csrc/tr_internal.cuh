@@ -125,15 +125,16 @@ struct TileTilt {
   int nq, nr;        // columns / rows of the window this tile can reach
 };
 
-// Back-projection coordinate starts of one staged tilt: the per-voxel steps
-// and, per warp w (wy = w % kTY, wz = w / kTY), the Q32.32 coordinates of the
-// warp's lane-0 first voxel, U0 + wy A1 + wz kNV A2 (V likewise), so that a
-// thread's start is one 64-bit multiply-add, W + lane A0.
+// Back-projection coordinate starts of one staged tilt, in Q9.23: the
+// per-voxel steps and, per warp w (wy = w % kTY, wz = w / kTY), the
+// coordinates of the warp's lane-0 first voxel, U0 + wy A1 + wz kNV A2
+// (V likewise), so that a thread's start is one 32-bit multiply-add,
+// u0 + lane du_x.
 struct WarpStarts {
-  long long A0, B0;
-  unsigned du, dv;   // Q9.23 steps along z
+  unsigned dux, dvx;  // steps along x (one lane)
+  unsigned du, dv;    // steps along z
   int jmin, check_rows;
-  long long Wu[kThreads / 32], Wv[kThreads / 32];
+  unsigned u0[kThreads / 32], v0[kThreads / 32];
 };
 
 // Forward-projection coordinate starts of one tilt: the x and z steps and,

@@ -89,6 +89,11 @@ __device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
 }
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) {
   return v < lo ? lo : (v > hi ? hi : v);
@@ -230,9 +235,10 @@ __device__ __forceinline__ void kahan_add(float &acc, float &c, float val) {
 
 // Window coordinates inside the z loop run in Q9.23 (32-bit): the integer
 // part is the window column/row (< 512), the 23 fraction bits are exactly the
-// float mantissa of 1 + dx.  Each thread's start is the exact Q32.32 value
-// truncated; the per-voxel step is rounded to 2^-23, so after the kNV - 1
-// steps of a thread the coordinate is within 8 * 2^-23 px of the exact one.
+// float mantissa of 1 + dx.  Each warp's start is the exact Q32.32 value
+// truncated and the lane and section steps are rounded to 2^-23, so a
+// thread's coordinates (31 lane steps at most, then kNV - 1 section steps)
+// stay within 24 * 2^-23 px of the exact ones.
 __device__ __forceinline__ unsigned q23(unsigned long long U) { return (unsigned)(U >> 9); }
 __device__ __forceinline__ unsigned q23_step(long long A) { return (unsigned)((A + 256) >> 9); }
 __device__ __forceinline__ float one_plus_frac23(unsigned u) {
@@ -248,11 +254,11 @@ __device__ __forceinline__ void fill_warp_starts(WarpStarts *ws, const TileTilt 
   const int i = tid / kW, w = tid % kW;
   const int wy = w % kTY, wz = w / kTY;
   const TiltGeo &g = geo[i];
-  ws[i].Wu[w] = tt[i].U0 + wy * g.A[1] + (long long)(wz * kNV) * g.A[2];
-  ws[i].Wv[w] = tt[i].V0 + wy * g.B[1] + (long long)(wz * kNV) * g.B[2];
+  ws[i].u0[w] = q23((unsigned long long)(tt[i].U0 + wy * g.A[1] + (long long)(wz * kNV) * g.A[2]));
+  ws[i].v0[w] = q23((unsigned long long)(tt[i].V0 + wy * g.B[1] + (long long)(wz * kNV) * g.B[2]));
   if (w == 0) {
-    ws[i].A0 = g.A[0];
-    ws[i].B0 = g.B[0];
+    ws[i].dux = q23_step(g.A[0]);
+    ws[i].dvx = q23_step(g.B[0]);
     ws[i].du = q23_step(g.A[2]);
     ws[i].dv = q23_step(g.B[2]);
     ws[i].jmin = tt[i].jmin;
@@ -276,18 +282,24 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
   }
   for (int i = 0; i < nc; ++i) {
     const WarpStarts &st = ws[i];
-    unsigned u = q23((unsigned long long)(st.Wu[w] + lane * st.A0));
+    unsigned u = st.u0[w] + lane * st.dux;
     const unsigned du = st.du;
     if (SEP) {
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)(i * kTY + wy) * fw;
+      // Two sections per step: the two sums advance in one f32x2 add (the
+      // same roundings as two scalar adds).
 #pragma unroll
-      for (int k = 0; k < kNV; ++k) {
-        const float2 t = T[u >> 23];
-        sum[k] += fmaf(one_plus_frac23(u), t.y, t.x);
+      for (int k = 0; k < kNV; k += 2) {
+        const float2 ta = T[u >> 23];
+        const float ra = fmaf(one_plus_frac23(u), ta.y, ta.x);
         u += du;
+        const float2 tb = T[u >> 23];
+        const float rb = fmaf(one_plus_frac23(u), tb.y, tb.x);
+        u += du;
+        unpack2(add2(pack2(sum[k], sum[k + 1]), pack2(ra, rb)), sum[k], sum[k + 1]);
       }
     } else {
-      unsigned v = q23((unsigned long long)(st.Wv[w] + lane * st.B0));
+      unsigned v = st.v0[w] + lane * st.dvx;
       const unsigned dv = st.dv;
       const float2 *T = reinterpret_cast<const float2 *>(tblv) + (size_t)i * per;
       const int jmin = st.jmin;
@@ -305,16 +317,29 @@ __device__ __forceinline__ void bp_accumulate(float (&acc)[kNV], float (&cmp)[kN
           v += dv;
         }
       } else {
+        // Two sections per step: the row interpolation and the sums of both
+        // run in f32x2 instructions (the same roundings as the scalar form
+        // sum += fma(dy, r1 - r0, r0)).
+        const f32x2 one2 = pack2(1.f, 1.f);
 #pragma unroll
-        for (int k = 0; k < kNV; ++k) {
-          const int q = (int)(u >> 23), r = (int)(v >> 23);
-          const float2 *e = T + r * fw + q;
-          const float2 t0 = e[0], t1 = e[fw];
-          const float f = one_plus_frac23(u);
-          const float r0 = fmaf(f, t0.y, t0.x), r1 = fmaf(f, t1.y, t1.x);
-          sum[k] += fmaf(one_plus_frac23(v) - 1.f, r1 - r0, r0);
-          u += du;
-          v += dv;
+        for (int k = 0; k < kNV; k += 2) {
+          float r0[2], r1[2], gy[2];
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int q = (int)(u >> 23), r = (int)(v >> 23);
+            const float2 *e = T + r * fw + q;
+            const float2 t0 = e[0], t1 = e[fw];
+            const float f = one_plus_frac23(u);
+            r0[h] = fmaf(f, t0.y, t0.x);
+            r1[h] = fmaf(f, t1.y, t1.x);
+            gy[h] = one_plus_frac23(v);
+            u += du;
+            v += dv;
+          }
+          const f32x2 R0 = pack2(r0[0], r0[1]);
+          const f32x2 d = sub2(pack2(r1[0], r1[1]), R0);
+          const f32x2 dy = sub2(pack2(gy[0], gy[1]), one2);
+          unpack2(add2(pack2(sum[k], sum[k + 1]), fma2(dy, d, R0)), sum[k], sum[k + 1]);
         }
       }
     }
