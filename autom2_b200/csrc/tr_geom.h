@@ -29,14 +29,36 @@ enum GeomStatus {
   GEOM_WINDOW,      // a window side exceeds kMaxWindow
 };
 
-// Most voxels of one forward-projection tile that can add to one window entry:
-// along x a row of voxels steps the detector column by |a1|, so at most
-// floor(2/|a1|) + 1 of them (+1 for fixed-point rounding) have their lower
-// column at q-1 or q; every (y, z) row of the tile may contribute.
-inline float fp_entry_bound(double min_a1) {
+// Most voxels of one section of a forward-projection tile (kFX x kTY voxels)
+// that can add to one window entry.  Entry (q, r) collects the voxels
+// whose detector coordinates (u, v) lie in [q-1, q+1) x [r-1, r+1), a 2 x 2
+// square; over one section (u, v) = M (x, y) + c with M = [[a1, a2], [b1, b2]],
+// so those voxels are the lattice points of the square's preimage, a
+// parallelogram of area 4/|det M| and perimeter 4 (|M^-1 e1| + |M^-1 e2|).  A
+// convex planar region of area A and perimeter P holds at most A + P/2 + 1
+// lattice points (Bokowski, Hadwiger and Wills, 1972); the square is widened
+// by 2^-16 px for the fixed-point coordinates and one point is added.
+inline double fp_section_bound(double a1, double a2, double b1, double b2) {
+  const double cap = (double)kFX * kTY;
+  const double det = a1 * b2 - a2 * b1;
+  if (!(std::fabs(det) > 1e-9)) return cap;
+  const double s = 2.0 + 1.0 / 65536.0;
+  // M^-1 = [[b2, -a2], [-b1, a1]] / det
+  const double c1 = std::hypot(b2, b1) / std::fabs(det), c2 = std::hypot(a2, a1) / std::fabs(det);
+  const double n = s * s / std::fabs(det) + s * (c1 + c2) + 2.0;
+  return std::min(cap, std::floor(n));
+}
+
+// Most voxels of one forward-projection tile that can add to one window
+// entry.  Separable windows hold one voxel row per window row: along x a row
+// steps the detector column by |a1|, so at most floor(2/|a1|) + 1 of its
+// voxels (+1 for fixed-point rounding) have their lower column at q-1 or q,
+// in each of the tile's kFTZ sections.  General geometry: kFTZ sections of at
+// most fp_section_bound voxels each (the largest over the tilts).
+inline float fp_entry_bound_sep(double min_a1) {
   double n = min_a1 > 2.0 / kFX ? std::floor(2.0 / min_a1) + 2.0 : (double)kFX;
   n = std::min(n, (double)kFX);
-  return (float)(n * kTY * kFTZ);
+  return (float)(n * kFTZ);
 }
 
 // Fills g[0..nt) and *out from [nt][8] coefficients; *bad_tilt names the
@@ -44,7 +66,7 @@ inline float fp_entry_bound(double min_a1) {
 inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
                            size_t smem_max, TiltGeo *g, GeomInfo *out, int *bad_tilt) {
   bool sep = true;
-  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30;
+  double span_u = 0, span_v = 0, fspan_u = 0, fspan_v = 0, min_a1 = 1e30, sect = 0;
   const double two32 = 4294967296.0;
   const double ext = std::max(std::max(nx, ny), th) + 64.0;
   *bad_tilt = -1;
@@ -70,6 +92,7 @@ inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
     if (reach_u > 1.0e9 || reach_v > 1.0e9) return GEOM_RANGE;
     if (!(k[5] == 0.0 && k[7] == 0.0 && k[6] == 1.0)) sep = false;
     min_a1 = std::min(min_a1, std::fabs(k[1]));
+    sect = std::max(sect, fp_section_bound(k[1], k[2], k[5], k[6]));
     span_u = std::max(span_u, std::fabs(k[1]) * (kTX - 1) + std::fabs(k[2]) * (kTY - 1) +
                                   std::fabs(k[3]) * (kTZ - 1));
     span_v = std::max(span_v, std::fabs(k[5]) * (kTX - 1) + std::fabs(k[6]) * (kTY - 1) +
@@ -86,8 +109,8 @@ inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
   // span whole 4-column groups, so that the flush adds 16-byte groups.
   out->ffw = ((int)std::ceil(fspan_u) + 4 + 3 + 3) & ~3;
   out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5;
+  out->nbound = sep ? fp_entry_bound_sep(min_a1) : (float)(sect * kFTZ);
   out->sep = sep;
-  out->nbound = fp_entry_bound(min_a1);
   out->fp_tilt_bytes = (size_t)out->ffw * out->ffh * sizeof(int);
   out->bp_tilt_bytes = (size_t)out->fw * out->fh * sizeof(float2);
   if (out->bp_tilt_bytes > smem_max || out->fp_tilt_bytes > smem_max) return GEOM_SMEM;

@@ -795,15 +795,16 @@ __global__ void __launch_bounds__(kThreads, std::is_same<IT, float>::value ? 4 :
 // compare-and-swap loop whose round trips left the kernel latency-bound).  The
 // tile's values are scaled by a power of two S chosen from the tile's largest
 // |voxel| so that no window entry can overflow: an entry collects at most
-// `nbound` voxel contributions (host bound from the x slope) of magnitude at
+// `nbound` voxel contributions (host bound: the lattice points of the entry's
+// 2 x 2 detector footprint in each section of the tile) of magnitude at
 // most max|v|, and S <= 2^30 / (nbound max|v|); also S <= 2^21 / max|v| so
 // every scaled contribution stays within the exact range of the float-shift
 // rounding (|x| < 2^22).  Per voxel and window row, the row's scaled value y
 // and its upper-column part t are each rounded to the nearest integer; the
 // upper tap adds round(t) and the lower round(y) - round(t), so a tap is off
-// by at most one quantum of max(nbound 2^-30, 2^-21) max|v| (nbound <= 768
-// for tilts within +-60 degrees: ~1e-6 of the tile's largest |v|, ~5e-7
-// where |a1| > 2/3) and a row's two taps by half a quantum together; the
+// by at most one quantum of max(nbound 2^-30, 2^-21) max|v| (nbound <= 512
+// for tilts within +-60 degrees and small in-plane rotations: ~5e-7 of the
+// tile's largest |v|) and a row's two taps by half a quantum together; the
 // sums are exact and independent of atomic order.  The arithmetic of a
 // lane's two voxels runs side by side in f32x2 instructions.
 // The flush converts back (x 1/S) and adds the in-image pixels to the global
