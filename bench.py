@@ -57,13 +57,13 @@ def peaks():
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum of the cfg1
 # geometry at half the lengths: stack 61 x 512^2, volume 512^2 x 128), scaled
 # by component to the full launch: voxel-side bytes x 8, detector-side bytes
-# x 4.  fp_kernel: 134.2 MB volume read x 8 + (66.7 MB read + 67.4 MB
-# written) x 4; bp_tma_kernel (SIRT): (134.2 MB volume read + 110.3 MB
-# written) x 8 + 240.4 MB detector-side reads x 4.  Captured with
+# x 4.  fp_kernel: 134.2 MB volume read x 8 + (66.6 MB read + 64.8 MB
+# written) x 4; bp_tma_kernel (SIRT): (134.2 MB volume read + 110.9 MB
+# written) x 8 + 229.2 MB detector-side reads x 4.  Captured with
 #   ncu --set full --clock-control none -k regex:<kernel> -s <n> -c 1 \
 #       python bench.py --kernels --scale 2 --iters 2
 # (fp_kernel: -s 4, the first timed iteration's; bp_tma_kernel: -s 1).
-TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": 1.6100e9, "bp_kernel": 2.9173e9}
+TRAFFIC_BYTES_PER_LAUNCH = {"fp_kernel": 1.5992e9, "bp_kernel": 2.8776e9}
 
 
 class ClockSampler:
