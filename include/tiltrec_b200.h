@@ -150,8 +150,6 @@ tr_status tr_forward_project(tr_ctx *ctx, const float *vol_dev, int z0, int nz,
 tr_status tr_sirt(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
                   int iters, float gamma, void *stream);
 
-/* SART, in place.  SART (main-mpi.cpp:578-612; main-mpiz.cpp:502-546),
- * CuSART / CuSARTZ (recon_y.cuh:35, recon_z.cuh:26). */
 /* SIRT (as tr_sirt) with an FP64 convergence gate.  Each iteration's
  * residual r = p - val/wt has its L2 norm summed in FP64 on the device
  * (fixed-order partial sums, so the norms repeat exactly) and read back; the
@@ -163,6 +161,9 @@ tr_status tr_sirt(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
 tr_status tr_sirt_gated(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
                         int max_iters, float gamma, double rel_tol,
                         double *norms_out, int *iters_done, void *stream);
+
+/* SART, in place.  SART (main-mpi.cpp:578-612; main-mpiz.cpp:502-546),
+ * CuSART / CuSARTZ (recon_y.cuh:35, recon_z.cuh:26). */
 tr_status tr_sart(tr_ctx *ctx, const float *proj_dev, float *vol_dev,
                   int iters, float gamma, void *stream);
 
@@ -269,6 +270,11 @@ tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
  * forward projection's float atomic adds.  Device memory: two reprojections
  * (ntilt*ny*nx floats each), the weights, and with a host volume three slabs
  * of depth*ny*nx floats. */
+tr_status tr_sirt_zslabs(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
+                         const float *scale_dev, int resid_dtype, float *vol,
+                         int vol_on_host, int iters, float gamma, int depth,
+                         void *stream);
+
 /* Deterministic forward projections for this context (on != 0; off by
  * default).  The splat's window flush then adds each pixel's contributions
  * as int64 fixed point at one launch-wide scale (the largest power of two S
@@ -281,11 +287,6 @@ tr_status tr_sirt_lp(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
  * the volume, int64 sums of twice the stack's bytes and a conversion pass per
  * forward projection.  Scheduler and tr_sirt_static calls are not affected. */
 tr_status tr_set_deterministic(tr_ctx *ctx, int on);
-
-tr_status tr_sirt_zslabs(tr_ctx *ctx, const void *proj_dev, int proj_dtype,
-                         const float *scale_dev, int resid_dtype, float *vol,
-                         int vol_on_host, int iters, float gamma, int depth,
-                         void *stream);
 
 /* SIRT over z-slabs from host buffers, the volume staying in host memory
  * (volumes larger than the device budget: TiltRecZ's managed-memory
