@@ -107,6 +107,13 @@ inline int derive_geometry(const double *coeff8, int nt, int nx, int ny, int th,
   out->fh = sep ? kTY : (int)std::ceil(span_v) + 5;
   // Forward windows start at a 4-column boundary (up to 3 extra columns) and
   // span whole 4-column groups, so that the flush adds 16-byte groups.
+  // Coverage: a tile's window starts at column floor(umin) - 1 - o (o <= 3,
+  // the alignment shift), and a voxel at fixed-point column u' (within eps
+  // << 1/2 px of its FP64 column) writes columns floor(u') - start and one
+  // more.  Over any tile position that index is at most
+  // floor(span + 2 eps) + 6 <= ceil(span) + 6 < ceil(span) + 7 <= ffw, with
+  // span = umax - umin <= fspan_u.  Rows start at floor(vmin) - 1 with no
+  // shift: at most ceil(span_v) + 3 < ffh.
   out->ffw = ((int)std::ceil(fspan_u) + 4 + 3 + 3) & ~3;
   out->ffh = sep ? kTY : (int)std::ceil(fspan_v) + 5;
   out->nbound = sep ? fp_entry_bound_sep(min_a1) : (float)(sect * kFTZ);

@@ -1027,7 +1027,10 @@ __device__ __forceinline__ void fp_tile(const FpArgs &a, int bx, int by, int bz,
       unsigned long long *ibase =
           DET ? a.ival + (size_t)(a.t0 + c0 + i) * a.tstride : nullptr;
       const float inv = s_inv;
-      const int ngq = (nq + 3) >> 2;
+      // Splat writes stay below column fw (the host's window width covers
+      // the tile's reach); nq comes from this tile's FP64 extremes, which
+      // rounding can put one column wider, so the flush stops at fw too.
+      const int ngq = (min(nq, fw) + 3) >> 2;
       for (int e = tid; e < nr * ngq; e += kThreads) {
         const int r = e / ngq, q = (e - r * ngq) << 2;
         const int4 v = *reinterpret_cast<const int4 *>(T + r * fw + q);
