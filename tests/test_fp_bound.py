@@ -39,6 +39,18 @@ extern "C" int probe_nbound(const double *c8, int nt, int nx, int ny, int th,
   *sep = gi.sep;
   return s;
 }
+extern "C" int probe_derive(const double *c8, int nt, int nx, int ny, int th, size_t smem,
+                            int *info, int *bad) {
+  static trb::TiltGeo g[1024];
+  if (nt > 1024) return -1;
+  trb::GeomInfo gi{};
+  const int s = trb::derive_geometry(c8, nt, nx, ny, th, smem, g, &gi, bad);
+  info[0] = gi.fw;
+  info[1] = gi.fh;
+  info[2] = gi.ffw;
+  info[3] = gi.ffh;
+  return s;
+}
 """
 
 
@@ -56,6 +68,8 @@ def probe(tmp_path_factory):
     lib.probe_nbound.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.POINTER(C.c_float), C.POINTER(C.c_int)]
     lib.probe_nbound.restype = C.c_int
+    lib.probe_derive.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+                                 C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int)]
 
     def nbound(c8, nx=1024, ny=1024, th=256):
         c8 = np.ascontiguousarray(c8, np.float64)
@@ -64,6 +78,14 @@ def probe(tmp_path_factory):
                               C.byref(nb), C.byref(sep))
         assert st == 0, f"derive_geometry refused the geometry ({st})"
         return float(nb.value), bool(sep.value)
+
+    def derive(c8, nx=1024, ny=1024, th=256, smem=200 * 1024):
+        c8 = np.ascontiguousarray(c8, np.float64)
+        info, bad = (C.c_int * 4)(), C.c_int()
+        st = lib.probe_derive(c8.ctypes.data_as(C.POINTER(C.c_double)), len(c8), nx, ny, th,
+                              C.c_size_t(smem), info, C.byref(bad))
+        return st, list(info), bad.value
+    nbound.derive = derive
     return nbound
 
 
@@ -144,3 +166,49 @@ def test_separable_bound_holds(probe, a1):
         assert sep
         got = max_entry_count(k, True, rng)
         assert got <= nb, f"a1 {sign * a1}: {got} voxels reach one entry, bound {nb}"
+
+
+# derive_geometry's status codes (tr_geom.h GeomStatus)
+GEOM_OK, GEOM_NONFINITE, GEOM_MAGNITUDE, GEOM_RANGE, GEOM_SMEM, GEOM_WINDOW = range(6)
+
+
+def test_geometry_refusals_name_the_tilt(probe):
+    """Coefficients the kernels cannot stage are refused with the reason,
+    and per-tilt failures name the offending tilt (window limits apply to the
+    whole series); the context and the no-allocation entry point map these to
+    TR_ERR_ARG (non-finite) or TR_ERR_UNSUPPORTED."""
+    rng = np.random.default_rng(5)
+    good = np.stack([general_tilt(rng, t, 0.5, 0.3) for t in np.linspace(-60, 60, 7)])
+    st, info, bad = probe.derive(good)
+    assert st == GEOM_OK and bad == -1
+    fw, fh, ffw, ffh = info
+    assert ffw % 4 == 0 and fw >= 32 and fh >= 5 and ffw >= 64 and ffh >= 5
+    cases = [
+        (3, 2, np.nan, GEOM_NONFINITE),
+        (4, 6, np.inf, GEOM_NONFINITE),
+        (2, 1, 2000.0, GEOM_MAGNITUDE),      # a slope above 1024
+        (5, 0, 3.0e9, GEOM_RANGE),           # detector columns beyond the int range
+        (1, 3, 40.0, GEOM_WINDOW),           # a tile reaching over 511 columns
+    ]
+    for t, i, v, want in cases:
+        k = good.copy()
+        k[t, i] = v
+        st, _, bad = probe.derive(k)
+        assert (st, bad) == (want, -1 if want == GEOM_WINDOW else t), (t, i, v)
+    # a window that fits the side limit but not the shared-memory budget
+    k = good.copy()
+    k[6, 3] = 6.0
+    assert probe.derive(k)[0] == GEOM_OK
+    st, _, bad = probe.derive(k, smem=4 * 1024)
+    assert (st, bad) == (GEOM_SMEM, -1)
+
+
+def test_separable_windows(probe):
+    """Separable geometry (b1 = b3 = 0, b2 = 1) keeps one window row per voxel
+    row: four rows whatever the tilt."""
+    k = np.array([[0.5, np.cos(a), 0.0, np.sin(a), 0.25, 0.0, 1.0, 0.0]
+                  for a in np.radians(np.linspace(-70, 70, 9))])
+    st, (fw, fh, ffw, ffh), _ = probe.derive(k)
+    assert st == GEOM_OK and fh == 4 and ffh == 4
+    span = np.abs(k[:, 1]) * 31 + np.abs(k[:, 3]) * 31
+    assert fw == int(np.ceil(span.max())) + 4
