@@ -56,3 +56,14 @@ def test_reference_arm_line_and_libraries():
     assert mapped, "the reference libraries were not loaded"
     assert all("/oracle/_ref/" in p for p in mapped), mapped
     assert not any("libtiltrec_b200" in p for p in mapped)
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun rank 0 alone times the reference; the other ranks exit 0
+    and print nothing."""
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "1"], cwd=ROOT, env=env,
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
