@@ -18,6 +18,17 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session")
+def cuda_include():
+    """The CUDA toolkit's include directory (beside the nvcc the library is
+    built with), for host-only test builds of headers that include it."""
+    from autom2_b200 import build
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(build.nvcc()))),
+                       "include")
+    assert os.path.exists(os.path.join(inc, "cuda_runtime.h")), inc
+    return inc
+
+
+@pytest.fixture(scope="session")
 def golden():
     with np.load(GOLDEN) as z:
         return {k: z[k] for k in z.files}

@@ -49,14 +49,14 @@ CAP = 1 << 16
 
 
 @pytest.fixture(scope="module")
-def spectrum(tmp_path_factory):
+def spectrum(tmp_path_factory, cuda_include):
     cxx = shutil.which("g++")
     assert cxx, "g++ is needed to compile the filter header for this test"
     d = tmp_path_factory.mktemp("rwprobe")
     (d / "p.cpp").write_text(PROBE)
     so = d / "p.so"
     subprocess.run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", f"-I{CSRC}",
-                    "-I/usr/local/cuda/include", str(d / "p.cpp"), "-o", str(so)], check=True)
+                    f"-I{cuda_include}", str(d / "p.cpp"), "-o", str(so)], check=True)
     lib = C.CDLL(str(so))
 
     def get(nx, smem_max=227 * 1024):

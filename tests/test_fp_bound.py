@@ -55,15 +55,14 @@ extern "C" int probe_derive(const double *c8, int nt, int nx, int ny, int th, si
 
 
 @pytest.fixture(scope="module")
-def probe(tmp_path_factory):
+def probe(tmp_path_factory, cuda_include):
     cxx = shutil.which("g++")
     assert cxx, "g++ is needed to compile the geometry header for this test"
     d = tmp_path_factory.mktemp("geomprobe")
     src, so = d / "probe.cpp", d / "probe.so"
     src.write_text(PROBE)
-    cuda_inc = Path("/usr/local/cuda/include")
     subprocess.run([cxx, "-O2", "-std=c++17", "-shared", "-fPIC", f"-I{CSRC}",
-                    f"-I{cuda_inc}", str(src), "-o", str(so)], check=True)
+                    f"-I{cuda_include}", str(src), "-o", str(so)], check=True)
     lib = C.CDLL(str(so))
     lib.probe_nbound.argtypes = [C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
                                  C.POINTER(C.c_float), C.POINTER(C.c_int)]
