@@ -53,6 +53,23 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError("build step failed: " + " ".join(cmd))
 
 
+def _tmp(out: str) -> str:
+    """A build output's temporary name, private to this process: ranks that
+    build at the same time (one process per GPU) each write their own file
+    and move it into place atomically, so none loads a half-written one."""
+    return f"{out}.tmp{os.getpid()}"
+
+
+def _build_to(out: str, cmd_for) -> None:
+    tmp = _tmp(out)
+    try:
+        _run(cmd_for(tmp))
+        os.replace(tmp, out)
+    finally:
+        if os.path.exists(tmp):
+            os.remove(tmp)
+
+
 def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
     srcs = [os.path.join(CSRC, s) for s in CU_SOURCES]
     deps = srcs + [os.path.join(CSRC, "tr_internal.cuh"), os.path.join(CSRC, "tr_geom.h"),
@@ -61,13 +78,14 @@ def build_lib(force: bool = False, verbose_ptxas: bool = False) -> str:
     if not force and _newer(LIB, deps):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    cmd = [nvcc(), *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-shared",
-           "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I", INCLUDE, "-I", CSRC,
-           "--expt-relaxed-constexpr", "-o", LIB + ".tmp", *srcs]
-    if verbose_ptxas:
-        cmd.insert(1, "-Xptxas=-v")
-    _run(cmd)
-    os.replace(LIB + ".tmp", LIB)
+    def cmd(tmp):
+        c = [nvcc(), *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-shared",
+             "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I", INCLUDE, "-I", CSRC,
+             "--expt-relaxed-constexpr", "-o", tmp, *srcs]
+        if verbose_ptxas:
+            c.insert(1, "-Xptxas=-v")
+        return c
+    _build_to(LIB, cmd)
     return LIB
 
 
@@ -82,18 +100,17 @@ def build_cli(force: bool = False) -> list[str]:
         out = os.path.join(BINDIR, name)
         deps = srcs + [os.path.join(CLI, "mrc_io.h"), LIB]
         if force or not _newer(out, deps):
-            _run(["g++", "-std=c++17", "-O2", f"-DTR_CLI_LAYOUT={layout}",
-                  f"-DTR_CLI_MPI_DIALECT={mpi}",
-                  "-I", INCLUDE, "-I", CLI, "-o", out + ".tmp", *srcs,
-                  "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
-            os.replace(out + ".tmp", out)
+            _build_to(out, lambda tmp, layout=layout, mpi=mpi: [
+                "g++", "-std=c++17", "-O2", f"-DTR_CLI_LAYOUT={layout}",
+                f"-DTR_CLI_MPI_DIALECT={mpi}", "-I", INCLUDE, "-I", CLI, "-o", tmp, *srcs,
+                "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
         outs.append(out)
     out = os.path.join(BINDIR, "resample")
     srcs_r = [os.path.join(CLI, "mrc_io.cpp"), os.path.join(CLI, "resample_cli.cpp")]
     if force or not _newer(out, srcs_r + [os.path.join(CLI, "mrc_io.h"), LIB]):
-        _run(["g++", "-std=c++17", "-O2", "-I", INCLUDE, "-I", CLI, "-o", out + ".tmp", *srcs_r,
-              "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
-        os.replace(out + ".tmp", out)
+        _build_to(out, lambda tmp: [
+            "g++", "-std=c++17", "-O2", "-I", INCLUDE, "-I", CLI, "-o", tmp, *srcs_r,
+            "-L", LIBDIR, "-ltiltrec_b200", "-Wl,-rpath,$ORIGIN/../lib"])
     outs.append(out)
     return outs
 

@@ -67,3 +67,18 @@ def test_only_rank_zero_works(exes, tmp_path):
     r = run(exes["TiltRec-cuda"], "-i", "missing.mrc", "-o", "x", "-t", "y", "-g", "0,0,0,4",
             "-m", "BPT", env=env)
     assert r.returncode == 0
+
+
+def test_concurrent_builds_leave_whole_binaries(exes):
+    """One process per GPU may build at the same time: each writes its own
+    temporary file and moves it into place, so two concurrent rebuilds leave
+    complete executables and no temporaries."""
+    import sys
+    code = "from autom2_b200 import build; build.build_cli(force=True)"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    procs = [subprocess.Popen([sys.executable, "-c", code], cwd=root) for _ in range(2)]
+    assert all(p.wait(timeout=300) == 0 for p in procs)
+    assert not [f for f in os.listdir(BIN) if ".tmp" in f]
+    for name in ("TiltRec-cuda", "TiltRecZ-cuda", "TiltRec-mpi", "TiltRecZ-mpi"):
+        r = run(os.path.join(BIN, name), "--help")
+        assert r.returncode == 0 and "--geometry" in r.stdout
